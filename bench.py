@@ -1,0 +1,342 @@
+"""Benchmark of the B200 TaiChi binary SpMV.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload rmat20|rmat20_selfloops|mesh|small]
+
+A step is one SpMV y = A x of the workload's matrix.  Default workload: the
+R-MAT scale-20 graph (1,048,576 rows, edge factor 16, a=0.499, b=c=0.001,
+seed 1, self-loops and duplicates removed), formatted by the GPU partitioner,
+FP32 x uniform in [-1, 1].
+
+`value` is SpMV GB/s (algorithmic bytes / device time per SpMV), inputs
+resident in HBM; the timed region replays a CUDA graph of back-to-back SpMVs
+that rotate over enough resident copies of the matrix and vectors (> 2x the
+126 MB L2) that every SpMV reads its operands from HBM.  `e2e` is the same
+metric through tc_spmv_host (pinned host x in, host y out, synchronous).
+With --impl reference the reference's CPU SpMV loop (main.cu:61-69, restated
+in the oracle) runs on all host cores on the same matrix.
+
+One JSON line on stdout (rank 0).  Multi-GPU (torchrun): independent replicas,
+one per GPU, max time over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpMV GB/s (% of HBM peak) at R-MAT scale 20"
+L2_BYTES = 126 * 2 ** 20
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_matrix(name):
+    from taichi_b200 import matgen
+    if name == "rmat20":
+        return matgen.rmat(20, 16, 0.499, 0.001, 0.001, seed=1), \
+            "R-MAT scale 20, ef 16, a=0.499 b=c=0.001, seed 1, no self-loops/duplicates"
+    if name == "rmat20_selfloops":
+        return matgen.rmat(20, 16, 0.499, 0.001, 0.001, seed=1, self_loops=True), \
+            "R-MAT scale 20 with self-loops kept (diagonal variant)"
+    if name == "mesh":
+        return matgen.mesh9(2048, 0.02, seed=2), "9-point stencil 2048^2, 2% rows permuted, seed 2"
+    if name == "small":
+        return matgen.diag_plus_random(65536, seed=0), "n=65536, diagonals -3..+4 + 10 random/row, seed 0"
+    raise SystemExit("unknown workload " + name)
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        rows = [r.split(", ") for r in out.strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(M, N, rp, col, x, seconds, threads):
+    """The reference's CPU SpMV loop (main.cu:61-69, restated in the oracle)
+    on a bounded sample: as many whole SpMVs as fit in `seconds`."""
+    import oracle
+    y = np.empty(M, np.float32)
+    nbytes = 4 * (M + 1) + 4 * int(rp[M]) + 4 * N + 4 * M
+    reps = 0
+    t0 = time.perf_counter()
+    while True:
+        if threads == 1:
+            oracle.lib().or_spmv_csr_f32_serial(M, rp, col, x, y)
+        else:
+            oracle.lib().or_spmv_csr_f32_omp(M, rp, col, x, y, threads)
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds:
+            break
+    return nbytes * reps / dt / 1e9, reps, dt
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU SpMV on all host cores."""
+    if rank != 0:
+        return
+    (M, N, rp, col), desc = make_matrix(args.workload)
+    x = np.random.default_rng(0).uniform(-1, 1, N).astype(np.float32)
+    threads = os.cpu_count() or 1
+    import oracle
+    y = np.empty(M, np.float32)
+    for _ in range(max(args.warmup, 3)):
+        oracle.lib().or_spmv_csr_f32_omp(M, rp, col, x, y, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.lib().or_spmv_csr_f32_omp(M, rp, col, x, y, threads)
+    dt = time.perf_counter() - t0
+    nbytes = 4 * (M + 1) + 4 * int(rp[M]) + 4 * N + 4 * M
+    val = nbytes * args.steps / dt / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic: " + desc,
+            "config": {"workload": args.workload + "_cpu_csr_spmv", "M": M, "N": N,
+                       "nnz": int(rp[M]), "bytes_per_spmv": nbytes},
+            "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": threads,
+                             "kind": "port",
+                             "sample": "%d whole SpMVs of the workload (main.cu:61-69 loop, "
+                                       "rows split over %d OpenMP threads)" % (args.steps, threads)},
+            "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import taichi_b200 as tc
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    (M, N, rp, col), desc = make_matrix(args.workload)
+    rng = np.random.default_rng(0)
+    x_host = rng.uniform(-1, 1, N).astype(np.float32)
+
+    # format build + GPU partition (timed once; not part of a step)
+    stream = torch.cuda.Stream(dev)
+    t0 = time.perf_counter()
+    prm = tc.params()
+    try:
+        plan0 = tc.Plan.from_csr(M, N, rp, col, prm=prm, stream=stream)
+        partition = "gpu"
+    except tc.TcError as e:
+        if "partitioner not available" not in str(e):
+            raise
+        plan0 = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(), partition=False, stream=stream)
+        partition = "skipped (plain CSR plan)"
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    info = plan0.info()
+    bytes_per = info["spmv_bytes"]
+    fmt = plan0.export()
+
+    # rotating resident copies so that every SpMV reads from HBM
+    ncopy = max(2, int(np.ceil(2.0 * L2_BYTES / bytes_per)))
+    ncopy = min(ncopy, 64)
+    plans = [plan0] + [tc.Plan.from_format(M, N, fmt, stream=stream) for _ in range(ncopy - 1)]
+    xs = [torch.from_numpy(x_host).to(dev) for _ in range(ncopy)]
+    ys = [torch.empty(M, dtype=torch.float32, device=dev) for _ in range(ncopy)]
+
+    # correctness guard on the benchmark input (FP64 oracle only in tests;
+    # here the integer-exact identity y(x=1) = row lengths)
+    ones = torch.ones(N, device=dev)
+    yo = torch.empty(M, device=dev)
+    plan0.spmv(ones, yo, stream=stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(yo.cpu().numpy(), np.diff(rp).astype(np.float32)), "SpMV check failed"
+
+    with torch.cuda.stream(stream):
+        for i in range(max(args.warmup, 3)):
+            plans[i % ncopy].spmv(xs[i % ncopy], ys[i % ncopy], stream=stream)
+    torch.cuda.synchronize()
+
+    # graph of G back-to-back SpMVs over the copies
+    G = min(args.steps, 512)
+    if G >= ncopy:
+        G -= G % ncopy
+
+    def capture(n):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            for i in range(n):
+                plans[i % ncopy].spmv(xs[i % ncopy], ys[i % ncopy], stream=torch.cuda.current_stream())
+        return g
+
+    g_main = capture(G)
+    reps, rem = divmod(args.steps, G)
+    g_rem = capture(rem) if rem else None
+    g_main.replay()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        g_main.replay()
+    if g_rem is not None:
+        g_rem.replay()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = ev0.elapsed_time(ev1)
+    cl = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    gbs = bytes_per / (ms_step * 1e-3) / 1e9 * world
+    peak, peak_kind = load_peaks()
+
+    # warm-L2 figure (same copy every time) for context
+    gw = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(gw, stream=stream):
+        for _ in range(256):
+            plan0.spmv(xs[0], ys[0], stream=torch.cuda.current_stream())
+    gw.replay()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    gw.replay()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    warm_ms = ev0.elapsed_time(ev1) / 256
+
+    # end to end through the public host API (pinned host buffers)
+    hx = torch.from_numpy(x_host).pin_memory()
+    hy = torch.empty(M, dtype=torch.float32).pin_memory()
+    e2e_steps = max(3, min(args.steps, 200))
+    for _ in range(3):
+        plan0.spmv_host(hx, hy, stream=stream)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        plan0.spmv_host(hx, hy, stream=stream)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_gbs = bytes_per / e2e_s / 1e9 * world
+
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get("spmv_tiles_kernel/" + args.workload)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, n, dt = cpu_baseline(M, N, rp, col, x_host, args.cpu_seconds, 1)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": "%d whole SpMVs in %.1f s (main.cu:61-69 serial FP32 loop)" % (n, dt)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(gbs, 2), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: " + desc,
+            "config": {"workload": args.workload + "_plain_hybrid_spmv", "M": M, "N": N,
+                       "nnz": int(rp[M]), "partition": partition,
+                       "dia_shapes": info["dia_shapes"], "num_negs": info["num_negs"],
+                       "nnz_csr": info["nnz_csr"], "tiles": info["ntiles"],
+                       "bytes_per_spmv": bytes_per, "format_build_s": round(build_s, 3),
+                       "partition_ms": info["partition_ms"],
+                       "l2": "rotating %d resident copies (%.0f MB) > 2x L2" % (
+                           ncopy, ncopy * bytes_per / 1e6),
+                       "warm_l2_gbs": round(bytes_per / (warm_ms * 1e-3) / 1e9, 1),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": round(gbs / world, 2), "peak": peak,
+                         "unit": "GB/s", "frac": round(gbs / world / peak, 4),
+                         "peak_kind": peak_kind + " hbm_gbs (copy)", "traffic": traffic},
+            "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 4 * N,
+                    "d2h_bytes_per_step": 4 * M, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": args.steps,
+            "clocks": cl,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    for p in plans:
+        p.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat20")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+/*
+ * taichi_b200.h -- C ABI of the B200-native TaiChi binary-SpMV library
+ * (libtaichi_b200.so).  Plain pointers, sizes and status codes only.
+ *
+ * The library also exports the reference's own C++ entry points with their
+ * original signatures (readMtx, partition_shapes, taichi_SpMV,
+ * free_taichi_new, ... -- see TaiChi.h in this directory), so a program
+ * written against the reference links against this library unchanged.
+ *
+ * Streams are passed as `void *` (a cudaStream_t; NULL = legacy default
+ * stream).  Device pointers are plain CUDA device addresses of the current
+ * device.  Every call returns a tc_status; tc_last_error() describes the last
+ * failure on the calling thread.
+ */
+#ifndef TAICHI_B200_H
+#define TAICHI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TC_API __attribute__((visibility("default")))
+#else
+#define TC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tc_status {
+    TC_OK = 0,
+    TC_ERR_INVALID = 1,     /* bad argument                                  */
+    TC_ERR_CUDA = 2,        /* a CUDA runtime call failed                    */
+    TC_ERR_ALLOC = 3,       /* device or host allocation failed              */
+    TC_ERR_IO = 4,          /* file could not be opened / parsed             */
+    TC_ERR_FORMAT = 5,      /* inconsistent sparse format                    */
+    TC_ERR_CAPACITY = 6,    /* a fixed capacity (pool, scratch) is exceeded  */
+    TC_ERR_TIMEOUT = 7,     /* a bounded device-side wait gave up            */
+    TC_ERR_UNSUPPORTED = 8  /* size or mode outside what the library handles */
+} tc_status;
+
+/* Partition and multiply parameters.  tc_params_default() gives the
+ * reference's hard-coded partition constants (morohutils.cu:140,191,239,242,
+ * 250; TaiChi.cu:379,757) and the library's default tile shape. */
+typedef struct tc_params {
+    int thumb_height;     /* thumbnail rows (512)                              */
+    int open_len;         /* length of the 30x1 / 1x30 opening lines (30)      */
+    int eye_size;         /* size of the diagonal opening element (5)          */
+    int min_contour;      /* contours with fewer points are dropped (80)       */
+    int min_shape_side;   /* shapes with a smaller side are skipped (1000)     */
+    double density;       /* a diagonal is dense if nnz/len >= density (0.6)   */
+    int tile_rows;        /* max rows per multiply tile (1024)                 */
+    int tile_nnz;         /* max CSR entries per multiply tile (4096)          */
+    int vector_threshold; /* tiles whose longest row exceeds this use a warp
+                             per row instead of a thread per row (32)          */
+    int flags;            /* TC_FLAG_*                                         */
+} tc_params;
+
+#define TC_FLAG_NO_PARTITION 0x1  /* skip the morphology: plain CSR plan      */
+#define TC_FLAG_KEEP_HOST    0x2  /* keep a host copy of the format (export)  */
+
+TC_API void tc_params_default(tc_params *p);
+
+TC_API const char *tc_last_error(void);
+TC_API const char *tc_status_string(tc_status s);
+
+/* ----------------------------------------------------------------------- */
+/* Resident plans: a formatted matrix kept in device memory.                */
+/* ----------------------------------------------------------------------- */
+typedef struct tc_plan tc_plan;
+
+/* Format view with the fields of the reference's TaiChi_new (TaiChi.h:45-60).
+ * All arrays are host arrays.  csrCol entries carry the sign bit
+ * ((col << 1) | add) when dia_shapes > 0 and are plain column indices when
+ * dia_shapes == 0. */
+typedef struct tc_format {
+    int dia_shapes, num_negs, dense_nnz, zero_elements, sparse_nnz;
+    int row_start, row_stop;
+    const int *xStart, *yStart, *xStop, *nDiasPtr, *neg_offsets;
+    const int *csrRow, *csrCol;
+} tc_format;
+
+/* Builds a plan from a binary CSR pattern (values are ignored except for the
+ * reference's FLT_MAX "already claimed" marker).  rowptr/col/val are host
+ * arrays unless on_device != 0.  The partition (thumbnail, morphology,
+ * contours, dense-diagonal extraction) runs on the GPU.  Replaces
+ * partition_shapes (TaiChi.cu:313-638) + the device upload of taichi_SpMV
+ * (TaiChi.cu:1357-1385). */
+TC_API tc_status tc_plan_create(int M, int N, int64_t nnz, const int *rowptr, const int *col,
+                         const float *val, int on_device, const tc_params *params,
+                         void *stream, tc_plan **out);
+
+/* Builds a plan from an already formatted matrix (host arrays). */
+TC_API tc_status tc_plan_from_format(int M, int N, const tc_format *fmt, const tc_params *params,
+                              void *stream, tc_plan **out);
+
+TC_API tc_status tc_plan_destroy(tc_plan *plan);
+
+typedef struct tc_plan_info {
+    int M, N;
+    int dia_shapes, num_negs, dense_nnz, zero_elements, sparse_nnz;
+    int row_start, row_stop;
+    int64_t nnz_input;        /* non-zeros of the input pattern               */
+    int64_t nnz_csr;          /* entries of the CSR remainder                 */
+    int ntiles, ntiles_vector, ntiles_long;
+    int64_t device_bytes;     /* HBM held by the plan                         */
+    int64_t spmv_bytes;       /* algorithmic bytes of one SpMV                */
+    double partition_ms;      /* GPU partition time at creation               */
+    int num_contours;         /* thumbnail contours kept (>= min_contour)      */
+} tc_plan_info;
+
+TC_API tc_status tc_plan_info_get(const tc_plan *plan, tc_plan_info *info);
+
+/* Copies the plan's format to caller-provided host arrays.  Pass NULL arrays
+ * to query sizes only (csrRow needs M+1 ints, csrCol nnz_csr ints, xStart/
+ * yStart/xStop dia_shapes ints, nDiasPtr dia_shapes+1, neg_offsets num_negs). */
+TC_API tc_status tc_plan_export(const tc_plan *plan, int *xStart, int *yStart, int *xStop,
+                         int *nDiasPtr, int *neg_offsets, int *csrRow, int *csrCol);
+
+/* The thumbnail-stage images of the last partition (5 x height x W bytes,
+ * 0/255: raster, filled, open-open, subtracted, eye-opened) and the kept
+ * shape corners (4 ints each).  Sizes are returned through *W / *ncorners. */
+TC_API tc_status tc_plan_thumbnail(const tc_plan *plan, unsigned char *stages, int *W,
+                            int *corners, int *ncorners);
+
+/* y = A x.  d_x: N floats, d_y: M floats, device memory.  Stream-ordered. */
+TC_API tc_status tc_spmv(const tc_plan *plan, const float *d_x, float *d_y, void *stream);
+
+/* Same multiply on host buffers: copies x in, multiplies, copies y out and
+ * waits.  Pinned host buffers give the full link bandwidth. */
+TC_API tc_status tc_spmv_host(const tc_plan *plan, const float *h_x, float *h_y, void *stream);
+
+/* Y = A X for k right-hand sides (1 <= k <= 64).  X is N x k row-major with
+ * leading dimension ldx >= k, Y is M x k with ldy >= k; device memory. */
+TC_API tc_status tc_spmm(const tc_plan *plan, const float *d_X, int ldx, int k, float *d_Y,
+                  int ldy, void *stream);
+
+/* ----------------------------------------------------------------------- */
+/* Thumbnail-level entry points of the GPU partitioner (device arrays).     */
+/* ----------------------------------------------------------------------- */
+
+/* Runs the thumbnail raster + morphology + contour tracing of getSdf
+ * (morohutils.cu:182-291) on a device CSR.  Writes up to max_corners shape
+ * corners (4 ints each, in OpenCV's contour order) to host memory and their
+ * count to *ncorners; *mF receives the thumbnail height (0 when the matrix
+ * has no thumbnail).  stages (optional, host) receives the 5 stage images. */
+TC_API tc_status tc_getsdf(int M, int N, const int *d_rowptr, const int *d_col, const tc_params *p,
+                    int *mF, int *W, int *corners, int max_corners, int *ncorners,
+                    unsigned char *stages, void *stream);
+
+/* Border following (findContours RETR_CCOMP / CHAIN_APPROX_NONE order) of a
+ * host H x W 0/nonzero image on the GPU.  Writes contour lengths (up to
+ * max_contours) and, for each, its first point and middle point (4 ints) to
+ * host memory.  Returns the number of contours in *ncontours. */
+TC_API tc_status tc_trace_contours(const unsigned char *img, int H, int W, int *lens, int *ends,
+                            int max_contours, int *ncontours);
+
+/* ----------------------------------------------------------------------- */
+/* Matrix Market reader (host).                                             */
+/* ----------------------------------------------------------------------- */
+
+/* Parses a Matrix Market coordinate file into a malloc'd CSR (free with
+ * tc_free).  Same result as readMtx (TaiChi.cu:120-278).  Returns TC_OK or
+ * TC_ERR_IO; *ref_code receives the reference's code (0, -1 open, -2 banner,
+ * -3 complex, -4 size line, -5 bad entry). */
+TC_API tc_status tc_read_mtx(const char *path, int *M, int *N, int64_t *nnz, int **rowptr,
+                      int **col, float **val, int *ref_code);
+TC_API void tc_free(void *p);
+
+/* ----------------------------------------------------------------------- */
+/* Batched form: many resident plans in one persistent launch.              */
+/* ----------------------------------------------------------------------- */
+typedef struct tc_batch tc_batch;
+
+/* Groups n plans; x[i] / y[i] are device vectors of plan i (fixed at creation
+ * so the launch can be captured in a CUDA graph). */
+TC_API tc_status tc_batch_create(int n, tc_plan *const *plans, const float *const *d_x,
+                          float *const *d_y, tc_batch **out);
+TC_API tc_status tc_batch_run(tc_batch *b, void *stream);              /* one launch  */
+TC_API tc_status tc_batch_graph_launch(tc_batch *b, void *stream);     /* graph replay */
+TC_API tc_status tc_batch_destroy(tc_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TAICHI_B200_H */

@@ -1,0 +1,271 @@
+"""taichi_b200 -- B200-native TaiChi binary SpMV.
+
+Python view of libtaichi_b200.so (the C ABI declared in include/taichi_b200.h),
+used by the tests and the benchmark.  The compute path is the CUDA library:
+if it is not built this module raises instead of falling back to anything.
+
+Device vectors may be given as torch CUDA tensors (float32, contiguous) or as
+raw device addresses (int).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtaichi_b200.so")
+_LIB = None
+
+TC_FLAG_NO_PARTITION = 0x1
+TC_FLAG_KEEP_HOST = 0x2
+
+_IP = C.POINTER(C.c_int)
+
+
+class TcError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("taichi_b200 status %d: %s" % (status, msg))
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("thumb_height", C.c_int), ("open_len", C.c_int), ("eye_size", C.c_int),
+                ("min_contour", C.c_int), ("min_shape_side", C.c_int), ("density", C.c_double),
+                ("tile_rows", C.c_int), ("tile_nnz", C.c_int), ("vector_threshold", C.c_int),
+                ("flags", C.c_int)]
+
+
+class Format(C.Structure):
+    _fields_ = [("dia_shapes", C.c_int), ("num_negs", C.c_int), ("dense_nnz", C.c_int),
+                ("zero_elements", C.c_int), ("sparse_nnz", C.c_int), ("row_start", C.c_int),
+                ("row_stop", C.c_int), ("xStart", _IP), ("yStart", _IP), ("xStop", _IP),
+                ("nDiasPtr", _IP), ("neg_offsets", _IP), ("csrRow", _IP), ("csrCol", _IP)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("M", C.c_int), ("N", C.c_int), ("dia_shapes", C.c_int), ("num_negs", C.c_int),
+                ("dense_nnz", C.c_int), ("zero_elements", C.c_int), ("sparse_nnz", C.c_int),
+                ("row_start", C.c_int), ("row_stop", C.c_int), ("nnz_input", C.c_int64),
+                ("nnz_csr", C.c_int64), ("ntiles", C.c_int), ("ntiles_vector", C.c_int),
+                ("ntiles_long", C.c_int), ("device_bytes", C.c_int64), ("spmv_bytes", C.c_int64),
+                ("partition_ms", C.c_double), ("num_contours", C.c_int)]
+
+
+# extern "C" symbols declared in include/taichi_b200.h (checked by the tests)
+EXPORTS = (
+    "tc_params_default", "tc_last_error", "tc_status_string", "tc_plan_create",
+    "tc_plan_from_format", "tc_plan_destroy", "tc_plan_info_get", "tc_plan_export",
+    "tc_plan_thumbnail", "tc_spmv", "tc_spmv_host", "tc_spmm", "tc_getsdf",
+    "tc_trace_contours", "tc_read_mtx", "tc_free", "tc_batch_create", "tc_batch_run",
+    "tc_batch_graph_launch", "tc_batch_destroy",
+)
+
+
+def lib():
+    """The loaded CUDA library; raises if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libtaichi_b200.so is not built (python -m taichi_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.tc_params_default.argtypes = [C.POINTER(Params)]
+        L.tc_params_default.restype = None
+        L.tc_last_error.restype = C.c_char_p
+        L.tc_status_string.restype = C.c_char_p
+        L.tc_status_string.argtypes = [C.c_int]
+        L.tc_plan_create.argtypes = [C.c_int, C.c_int, C.c_int64, vp, vp, vp, C.c_int,
+                                     C.POINTER(Params), vp, C.POINTER(vp)]
+        L.tc_plan_from_format.argtypes = [C.c_int, C.c_int, C.POINTER(Format),
+                                          C.POINTER(Params), vp, C.POINTER(vp)]
+        L.tc_plan_destroy.argtypes = [vp]
+        L.tc_plan_info_get.argtypes = [vp, C.POINTER(PlanInfo)]
+        L.tc_plan_export.argtypes = [vp] + [vp] * 7
+        L.tc_plan_thumbnail.argtypes = [vp, vp, _IP, vp, _IP]
+        L.tc_spmv.argtypes = [vp, vp, vp, vp]
+        L.tc_spmv_host.argtypes = [vp, vp, vp, vp]
+        L.tc_spmm.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp]
+        L.tc_getsdf.argtypes = [C.c_int, C.c_int, vp, vp, C.POINTER(Params), _IP, _IP, vp,
+                                C.c_int, _IP, vp, vp]
+        L.tc_trace_contours.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, _IP]
+        L.tc_read_mtx.argtypes = [C.c_char_p, _IP, _IP, C.POINTER(C.c_int64), C.POINTER(_IP),
+                                  C.POINTER(_IP), C.POINTER(C.POINTER(C.c_float)), _IP]
+        L.tc_free.argtypes = [vp]
+        L.tc_batch_create.argtypes = [C.c_int, vp, vp, vp, C.POINTER(vp)]
+        L.tc_batch_run.argtypes = [vp, vp]
+        L.tc_batch_graph_launch.argtypes = [vp, vp]
+        L.tc_batch_destroy.argtypes = [vp]
+        _LIB = L
+    return _LIB
+
+
+def check(status):
+    if status != 0:
+        raise TcError(status, lib().tc_last_error().decode(errors="replace"))
+
+
+def params(**over):
+    p = Params()
+    lib().tc_params_default(C.byref(p))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    """Device address of a torch tensor / raw int, or host address of numpy."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous(), "tensor must be contiguous"
+        return a.data_ptr()
+    raise TypeError("unsupported array type %r" % type(a))
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+def read_mtx(path):
+    """Matrix Market -> (M, N, rowptr, col, val) numpy arrays (readMtx)."""
+    L = lib()
+    M, N, nnz, code = C.c_int(), C.c_int(), C.c_int64(), C.c_int()
+    rp, ci, va = _IP(), _IP(), C.POINTER(C.c_float)()
+    st = L.tc_read_mtx(path.encode(), C.byref(M), C.byref(N), C.byref(nnz), C.byref(rp),
+                       C.byref(ci), C.byref(va), C.byref(code))
+    if st != 0:
+        raise TcError(st, "%s (reference code %d)" % (L.tc_last_error().decode(), code.value))
+    m, z = M.value, nnz.value
+    out = (m, N.value, np.ctypeslib.as_array(rp, shape=(m + 1,)).copy(),
+           np.ctypeslib.as_array(ci, shape=(max(z, 1),))[:z].copy(),
+           np.ctypeslib.as_array(va, shape=(max(z, 1),))[:z].copy())
+    for p in (rp, ci, va):
+        L.tc_free(C.cast(p, C.c_void_p))
+    return out
+
+
+class Plan:
+    """A matrix formatted and resident in device memory (tc_plan)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    # -- construction -------------------------------------------------------
+    @classmethod
+    def from_csr(cls, M, N, rowptr, col, val=None, prm=None, on_device=False, stream=None,
+                 partition=True, keep_host=False):
+        p = prm or params()
+        if not partition:
+            p.flags |= TC_FLAG_NO_PARTITION
+        if keep_host:
+            p.flags |= TC_FLAG_KEEP_HOST
+        keep = []
+        if not on_device:
+            rowptr = np.ascontiguousarray(rowptr, np.int32)
+            col = np.ascontiguousarray(col, np.int32)
+            keep += [rowptr, col]
+            if val is not None:
+                val = np.ascontiguousarray(val, np.float32)
+                keep.append(val)
+        nnz = int(rowptr[M]) if not on_device else int(rowptr[M].item())
+        h = C.c_void_p()
+        check(lib().tc_plan_create(M, N, nnz, _ptr(rowptr), _ptr(col), _ptr(val),
+                                   1 if on_device else 0, C.byref(p), _stream(stream),
+                                   C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_format(cls, M, N, fmt, prm=None, stream=None):
+        """fmt: dict with the TaiChi_new fields (numpy arrays)."""
+        f = Format()
+        keep = {}
+        for k in ("dia_shapes", "num_negs", "dense_nnz", "zero_elements", "sparse_nnz",
+                  "row_start", "row_stop"):
+            setattr(f, k, int(fmt[k]))
+        for k in ("xStart", "yStart", "xStop", "nDiasPtr", "neg_offsets", "csrRow", "csrCol"):
+            a = fmt.get(k)
+            if a is None:
+                continue
+            a = np.ascontiguousarray(a, np.int32)
+            if a.size == 0:
+                a = np.zeros(1, np.int32)
+            keep[k] = a
+            setattr(f, k, a.ctypes.data_as(_IP))
+        h = C.c_void_p()
+        check(lib().tc_plan_from_format(M, N, C.byref(f), C.byref(prm or params()),
+                                        _stream(stream), C.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            lib().tc_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- queries ------------------------------------------------------------
+    def info(self):
+        i = PlanInfo()
+        check(lib().tc_plan_info_get(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in PlanInfo._fields_}
+
+    def export(self):
+        """Host copy of the plan's format as a dict (TaiChi_new fields)."""
+        i = self.info()
+        s, ng, M = i["dia_shapes"], i["num_negs"], i["M"]
+        arrs = {"xStart": np.zeros(max(s, 1), np.int32), "yStart": np.zeros(max(s, 1), np.int32),
+                "xStop": np.zeros(max(s, 1), np.int32), "nDiasPtr": np.zeros(s + 1, np.int32),
+                "neg_offsets": np.zeros(max(ng, 1), np.int32),
+                "csrRow": np.zeros(M + 1, np.int32),
+                "csrCol": np.zeros(max(i["nnz_csr"], 1), np.int32)}
+        check(lib().tc_plan_export(self._h, *[arrs[k].ctypes.data for k in
+                                              ("xStart", "yStart", "xStop", "nDiasPtr",
+                                               "neg_offsets", "csrRow", "csrCol")]))
+        d = {k: i[k] for k in ("dia_shapes", "num_negs", "dense_nnz", "zero_elements",
+                               "sparse_nnz", "row_start", "row_stop")}
+        d["xStart"], d["yStart"], d["xStop"] = arrs["xStart"][:s], arrs["yStart"][:s], arrs["xStop"][:s]
+        d["nDiasPtr"] = arrs["nDiasPtr"] if s > 0 else np.zeros(0, np.int32)
+        d["neg_offsets"] = arrs["neg_offsets"][:ng]
+        d["csrRow"] = arrs["csrRow"]
+        d["csrCol"] = arrs["csrCol"][:i["nnz_csr"]]
+        return d
+
+    def thumbnail(self, height=512):
+        W, n = C.c_int(), C.c_int()
+        check(lib().tc_plan_thumbnail(self._h, None, C.byref(W), None, C.byref(n)))
+        corners = np.zeros((max(n.value, 1), 4), np.int32)
+        st = np.zeros((5, height, max(W.value, 1)), np.uint8)
+        check(lib().tc_plan_thumbnail(self._h, st.ctypes.data, C.byref(W), corners.ctypes.data,
+                                      C.byref(n)))
+        return corners[:n.value], st if W.value else None
+
+    # -- multiply -----------------------------------------------------------
+    def spmv(self, x, y, stream=None):
+        check(lib().tc_spmv(self._h, _ptr(x), _ptr(y), _stream(stream)))
+
+    def spmv_host(self, x, y, stream=None):
+        check(lib().tc_spmv_host(self._h, _ptr(x), _ptr(y), _stream(stream)))
+
+    def spmm(self, X, Y, k=None, ldx=None, ldy=None, stream=None):
+        if k is None:
+            k = X.shape[1]
+        ldx = ldx or X.shape[1]
+        ldy = ldy or Y.shape[1]
+        check(lib().tc_spmm(self._h, _ptr(X), ldx, k, _ptr(Y), ldy, _stream(stream)))

@@ -1,0 +1,138 @@
+// tc_internal.h -- shared definitions of libtaichi_b200 (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "taichi_b200.h"
+
+namespace tc {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char *fmt, ...);
+tc_status fail(tc_status s, const char *fmt, ...);
+
+#define TC_CUDA(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess)                                                     \
+            return ::tc::fail(TC_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__,     \
+                              #call, cudaGetErrorString(e_));                      \
+    } while (0)
+
+#define TC_CHECK(st)                                                               \
+    do {                                                                           \
+        tc_status s_ = (st);                                                       \
+        if (s_ != TC_OK) return s_;                                                \
+    } while (0)
+
+// ------------------------------------------------------------- tile plan
+// A multiply tile is a run of consecutive rows processed by one CTA.
+enum TileKind : int {
+    TILE_SCALAR = 0,   // thread per row, CSR entries staged in shared memory
+    TILE_VECTOR = 1,   // warp per row, CSR entries staged in shared memory
+    TILE_LONG = 2      // one long row, CTA-wide reduction straight from HBM
+};
+
+struct Tile {          // 16 bytes, read once per CTA
+    int row0;          // first row
+    int nz0;           // first CSR entry (rowptr[row0])
+    int nnz;           // CSR entries of the tile
+    int nrows_kind;    // nrows | kind << 28
+};
+
+__host__ __device__ inline int tile_nrows(const Tile &t) { return t.nrows_kind & 0x0fffffff; }
+__host__ __device__ inline int tile_kind(const Tile &t) { return (t.nrows_kind >> 28) & 0xf; }
+
+// Compile-time limits of the tile kernel (shared-memory staging buffers).
+constexpr int kBlock = 256;           // threads per CTA
+constexpr int kMaxTileRows = 2040;    // rows staged per tile (rows+1 <= 8*kBlock)
+constexpr int kMaxTileNnz = 8192;     // CSR entries staged per tile
+
+// Everything a multiply kernel needs about one plan (passed by value).
+struct DevPlan {
+    const int *rowptr;      // M+1
+    const int *cols;        // nnz_csr (signed (col<<1|add) when hybrid)
+    const Tile *tiles;      // ntiles
+    const int4 *shapes;     // dia_shapes: {xStart, xStop, yStart, Msub}
+    const int2 *shape_dias; // dia_shapes: {first offset, end offset}
+    const int *offsets;     // num_negs
+    int M, N, ntiles, dia_shapes, row_start, row_stop, hybrid;
+    int max_span;           // widest offset span of any shape (max-min)
+    int rows_cap, nnz_cap;  // tile limits the plan was built with
+};
+
+struct tc_plan_impl;
+
+}  // namespace tc
+
+// Opaque plan (the public tc_plan).
+struct tc_plan {
+    int M = 0, N = 0;
+    tc_params params{};
+    // format scalars (TaiChi_new)
+    int dia_shapes = 0, num_negs = 0, dense_nnz = 0, zero_elements = 0, sparse_nnz = 0;
+    int row_start = 0, row_stop = 0;
+    int64_t nnz_input = 0, nnz_csr = 0;
+    int hybrid = 0;
+    // device arrays (one allocation, `dev`)
+    void *dev = nullptr;
+    size_t dev_bytes = 0;
+    int *d_rowptr = nullptr, *d_cols = nullptr, *d_offsets = nullptr;
+    tc::Tile *d_tiles = nullptr;
+    int4 *d_shapes = nullptr;
+    int2 *d_shape_dias = nullptr;
+    int ntiles = 0, ntiles_vector = 0, ntiles_long = 0;
+    int max_span = 0;
+    // host copies of the small format arrays (always) and optionally the CSR
+    std::vector<int> h_xStart, h_yStart, h_xStop, h_nDiasPtr, h_offsets;
+    std::vector<int> h_rowptr, h_cols;   // only with TC_FLAG_KEEP_HOST
+    // partition diagnostics
+    double partition_ms = 0.0;
+    int thumb_W = 0, thumb_H = 0;
+    std::vector<unsigned char> thumb_stages;   // 5*H*W when kept
+    std::vector<int> corners;                   // 4 per kept contour
+    // device staging for tc_spmv_host
+    float *d_xbuf = nullptr, *d_ybuf = nullptr;
+
+    tc::DevPlan dev_plan() const;
+    int64_t spmv_bytes() const;
+};
+
+namespace tc {
+// Builds the tiles + device format from host arrays of an already formatted
+// matrix (csrRow has M+1 entries).  Shared by every plan constructor.
+tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol,
+                      cudaStream_t stream);
+// Host tile planner (row-length histogram -> tile kinds).
+void plan_tiles(const int *rowptr, int M, const tc_params &prm, std::vector<Tile> &tiles,
+                int *nvec, int *nlong);
+// Launch of the multiply kernel for one plan.
+tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
+tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,
+                      cudaStream_t s);
+size_t spmv_smem_bytes(int rows_cap, int nnz_cap, int max_span);
+
+// GPU partitioner: device CSR in, format (host vectors) out.
+struct PartitionOut {
+    int dia_shapes = 0, num_negs = 0, dense_nnz = 0, zero_elements = 0, sparse_nnz = 0;
+    int row_start = 0, row_stop = 0;
+    std::vector<int> xStart, yStart, xStop, nDiasPtr, offsets;
+    // device CSR remainder (allocated here with cudaMalloc; caller frees)
+    int *d_rowptr = nullptr, *d_cols = nullptr;
+    int64_t nnz_csr = 0;
+    bool aliases_input = false;      // dense_nnz == 0: the input CSR is the format
+    int thumb_W = 0, thumb_H = 0, ncontours = 0;
+    std::vector<int> corners;
+    std::vector<unsigned char> stages;
+    std::vector<unsigned char> claimed;   // per input entry, when requested
+    double ms = 0.0;
+};
+tc_status gpu_partition(int M, int N, int64_t nnz, const int *d_rowptr, const int *d_col,
+                        const float *d_val, const tc_params &prm, bool keep_stages,
+                        bool want_claimed, cudaStream_t s, PartitionOut &out);
+}  // namespace tc

@@ -1,0 +1,92 @@
+"""SpMM (1..64 right-hand sides) and the batched persistent launch, against
+the FP64 oracle and against the single-plan multiply (bit-identical)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.golden import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def dev_t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+@pytest.mark.parametrize("k", [1, 2, 7, 32, 33, 64])
+@pytest.mark.parametrize("name", ["band_holes", "multi_shape", "cfg1_small"])
+def test_spmm(tc, dev, k, name):
+    import torch
+    case = next(c for c in cases.MATRIX_CASES if c["name"] == name)
+    M, N, rp, col = cases.matrix(case)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    plan = tc.Plan.from_format(M, N, fmt)
+    rng = np.random.default_rng(k)
+    X = rng.integers(-8, 9, (N, k)).astype(np.float32)
+    Y = torch.full((M, k), float("nan"), device=dev)
+    plan.spmm(dev_t(X, dev), Y)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(Y.cpu().numpy().astype(np.float64),
+                                  oracle.spmm_csr_f64(M, rp, col, X.astype(np.float64)))
+    # column j of SpMM == SpMV of column j for integer X (exact either way)
+    Xf = rng.uniform(-1, 1, (N, k)).astype(np.float32)
+    plan.spmm(dev_t(Xf, dev), Y)
+    torch.cuda.synchronize()
+    Y64 = oracle.spmm_csr_f64(M, rp, col, Xf.astype(np.float64))
+    rel = np.linalg.norm(Y.cpu().numpy() - Y64) / np.linalg.norm(Y64)
+    print("spmm %s k=%d rel err %.2e" % (name, k, rel))
+    assert rel <= 1e-5
+
+
+def test_spmm_strided(tc, dev):
+    import torch
+    case = cases.MATRIX_CASES[2]
+    M, N, rp, col = cases.matrix(case)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    plan = tc.Plan.from_format(M, N, fmt)
+    X = np.random.default_rng(0).integers(-8, 9, (N, 40)).astype(np.float32)
+    Y = torch.zeros((M, 48), device=dev)
+    plan.spmm(dev_t(X, dev), Y, k=20, ldx=40, ldy=48)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(Y.cpu().numpy()[:, :20].astype(np.float64),
+                                  oracle.spmm_csr_f64(M, rp, col, X[:, :20].astype(np.float64)))
+    assert not Y.cpu().numpy()[:, 20:].any()
+
+
+def test_batch_identical_to_solo(tc, dev):
+    import ctypes as C
+    import torch
+    names = ["band_holes", "two_segments", "multi_shape", "cfg1_small", "wide_band", "overlap"]
+    plans, xs, ys, solo = [], [], [], []
+    rng = np.random.default_rng(5)
+    for nm in names:
+        case = next(c for c in cases.MATRIX_CASES if c["name"] == nm)
+        M, N, rp, col = cases.matrix(case)
+        fmt, _ = oracle.partition(M, N, rp, col)
+        p = tc.Plan.from_format(M, N, fmt)
+        x = torch.from_numpy(rng.uniform(-1, 1, N).astype(np.float32)).to(dev)
+        y = torch.empty(M, device=dev)
+        p.spmv(x, y)
+        torch.cuda.synchronize()
+        solo.append(y.clone())
+        y.fill_(float("nan"))
+        plans.append(p); xs.append(x); ys.append(y)
+    n = len(plans)
+    H = (C.c_void_p * n)(*[p.handle.value for p in plans])
+    X = (C.c_void_p * n)(*[x.data_ptr() for x in xs])
+    Yp = (C.c_void_p * n)(*[y.data_ptr() for y in ys])
+    b = C.c_void_p()
+    tc.check(tc.lib().tc_batch_create(n, H, X, Yp, C.byref(b)))
+    tc.check(tc.lib().tc_batch_run(b, None))
+    torch.cuda.synchronize()
+    for y, s in zip(ys, solo):
+        assert torch.equal(y, s)
+    for y in ys:
+        y.fill_(float("nan"))
+    for _ in range(3):
+        tc.check(tc.lib().tc_batch_graph_launch(b, None))
+    torch.cuda.synchronize()
+    for y, s in zip(ys, solo):
+        assert torch.equal(y, s)
+    tc.check(tc.lib().tc_batch_destroy(b))

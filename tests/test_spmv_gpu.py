@@ -1,0 +1,154 @@
+"""Parity of the CUDA multiply with the oracle (FP64 CPU), through the C ABI.
+
+Bar: bit-exact y for integer-valued x in [-8, 8]; for FP32 x uniform in
+[-1, 1], normwise relative error <= 1e-5 against FP64 and, per row,
+|y - y64| <= 1e-5 * (sum of |terms| the row adds, holes counted twice)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.golden import cases
+from taichi_b200 import matgen
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def to_dev(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def run_spmv(plan, x, M, dev):
+    import torch
+    xd = to_dev(x.astype(np.float32), dev)
+    y = torch.full((M,), float("nan"), dtype=torch.float32, device=dev)
+    plan.spmv(xd, y)
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+def abs_terms(fmt, M, N, rp, col, x):
+    """Sum of |terms| a row of the format adds: the pattern plus the holes
+    twice (once on the dense diagonal, once subtracted)."""
+    a = oracle.spmv_csr_f64(M, rp, col, np.abs(x))
+    if fmt["dense_nnz"] > 0 and len(fmt["csrCol"]):
+        cc = fmt["csrCol"]
+        holes = (cc & 1) == 0
+        rows = np.repeat(np.arange(M), np.diff(fmt["csrRow"]))
+        a += 2 * np.bincount(rows[holes], weights=np.abs(x[cc[holes] >> 1]), minlength=M)
+    return a
+
+
+def check_plan(plan, fmt, M, N, rp, col, dev, label):
+    rng = np.random.default_rng(7)
+    # integer x: every partial sum is an exact float
+    xi = rng.integers(-8, 9, N).astype(np.float64)
+    yi = run_spmv(plan, xi, M, dev)
+    want = oracle.spmv_csr_f64(M, rp, col, xi)
+    np.testing.assert_array_equal(yi.astype(np.float64), want, err_msg=label + " integer x")
+    # x == 1 (the reference's own check, main.cu:53-86): y = row lengths
+    y1 = run_spmv(plan, np.ones(N), M, dev)
+    np.testing.assert_array_equal(y1, np.diff(rp).astype(np.float32), err_msg=label + " x=1")
+    # random FP32 x
+    xf = rng.uniform(-1, 1, N).astype(np.float32)
+    yf = run_spmv(plan, xf, M, dev).astype(np.float64)
+    y64 = oracle.spmv_csr_f64(M, rp, col, xf.astype(np.float64))
+    nrm = np.linalg.norm(y64)
+    rel = np.linalg.norm(yf - y64) / nrm if nrm > 0 else np.linalg.norm(yf)
+    bound = abs_terms(fmt, M, N, rp, col, xf.astype(np.float64))
+    roww = np.max(np.abs(yf - y64) / np.maximum(bound, 1e-30)) if M else 0.0
+    print("%s: normwise rel err %.2e, max row-wise err %.2e" % (label, rel, roww))
+    assert rel <= TOL and roww <= TOL, (label, rel, roww)
+
+
+PARTITION_CASES = [c for c in cases.MATRIX_CASES if c["name"] not in ("mesh2048",)]
+
+
+@pytest.mark.parametrize("case", PARTITION_CASES, ids=[c["name"] for c in PARTITION_CASES])
+def test_spmv_oracle_format(tc, dev, case):
+    """Plans built from the oracle's partition (pinned to the reference)."""
+    M, N, rp, col = cases.matrix(case)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    plan = tc.Plan.from_format(M, N, fmt)
+    check_plan(plan, fmt, M, N, rp, col, dev, case["name"])
+    plan.close()
+
+
+@pytest.mark.parametrize("case", PARTITION_CASES[:8], ids=[c["name"] for c in PARTITION_CASES[:8]])
+def test_spmv_plain_csr(tc, dev, case):
+    M, N, rp, col = cases.matrix(case)
+    plan = tc.Plan.from_csr(M, N, rp, col, partition=False)
+    fmt = dict(dense_nnz=0, csrRow=rp, csrCol=col)
+    check_plan(plan, fmt, M, N, rp, col, dev, case["name"] + "/plain")
+    plan.close()
+
+
+def csr_from_lengths(lengths, N, seed):
+    rng = np.random.default_rng(seed)
+    rp = np.zeros(len(lengths) + 1, np.int64)
+    np.cumsum(lengths, out=rp[1:])
+    col = rng.integers(0, N, int(rp[-1])).astype(np.int32)
+    return rp.astype(np.int32), col
+
+
+@pytest.mark.parametrize("tile", [(1024, 4096), (1, 1), (3, 7), (2040, 8192), (64, 100)])
+def test_tile_kinds_and_edges(tc, dev, tile):
+    """Empty rows, long rows (CTA per row), medium rows (warp per row),
+    duplicates, and extreme tile limits."""
+    rng = np.random.default_rng(11)
+    lengths = np.concatenate([np.zeros(300, int), rng.integers(0, 3, 2000), [5000, 0, 9000],
+                              rng.integers(30, 200, 50), [1], np.zeros(5, int), [70000],
+                              rng.integers(0, 12, 3000)])
+    M, N = len(lengths), 7000
+    rp, col = csr_from_lengths(lengths, N, 3)
+    prm = tc.params(tile_rows=tile[0], tile_nnz=tile[1])
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=prm, partition=False)
+    info = plan.info()
+    assert info["ntiles_long"] >= 1 if tile[1] < 9000 else True
+    check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "edges%s" % (tile,))
+
+
+def test_empty_and_tiny(tc, dev):
+    import torch
+    # no non-zeros at all
+    M, N = 1000, 500
+    rp = np.zeros(M + 1, np.int32)
+    plan = tc.Plan.from_csr(M, N, rp, np.zeros(0, np.int32), partition=False)
+    assert not run_spmv(plan, np.ones(N), M, dev).any()
+    # one row, one column
+    plan = tc.Plan.from_csr(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32),
+                            partition=False)
+    assert run_spmv(plan, np.array([3.0]), 1, dev)[0] == 3.0
+    # M == 0
+    plan = tc.Plan.from_csr(0, 5, np.zeros(1, np.int32), np.zeros(0, np.int32), partition=False)
+    plan.spmv(torch.ones(5, device=dev), torch.empty(0, device=dev))
+
+
+def test_hybrid_without_csr_remainder(tc, dev):
+    """All non-zeros on hole-free dense diagonals: the reference leaves the CSR
+    unallocated and its kernel reads an invalid pointer; here y is exact."""
+    M, N, rp, col = matgen.segments(20000, [(0, 20000, 0, 1, 1.0)], noise=0, seed=1)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    assert fmt["dia_shapes"] == 1 and fmt["zero_elements"] + fmt["sparse_nnz"] == 0
+    plan = tc.Plan.from_format(M, N, fmt)
+    check_plan(plan, fmt, M, N, rp, col, dev, "no-remainder")
+
+
+def test_spmv_host_e2e(tc, dev):
+    M, N, rp, col = cases.matrix(cases.MATRIX_CASES[1])
+    fmt, _ = oracle.partition(M, N, rp, col)
+    plan = tc.Plan.from_format(M, N, fmt)
+    x = np.random.default_rng(2).integers(-8, 9, N).astype(np.float32)
+    y = np.zeros(M, np.float32)
+    plan.spmv_host(x, y)
+    np.testing.assert_array_equal(y.astype(np.float64), oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64)))
+
+
+def test_format_rejected(tc):
+    M, N = 10, 10
+    rp = np.array([0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10], np.int32)
+    bad = dict(dia_shapes=0, num_negs=0, dense_nnz=0, zero_elements=0, sparse_nnz=10,
+               row_start=0, row_stop=0, csrRow=rp, csrCol=np.full(10, 12, np.int32))
+    with pytest.raises(tc.TcError):
+        tc.Plan.from_format(M, N, bad)
