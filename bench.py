@@ -212,7 +212,8 @@ def run_ours(args, rank, world, local_rank):
     g_main = capture(G)
     reps, rem = divmod(args.steps, G)
     g_rem = capture(rem) if rem else None
-    g_main.replay()
+    with torch.cuda.stream(stream):
+        g_main.replay()
     torch.cuda.synchronize()
 
     clocks = Clocks(local_rank)
@@ -223,12 +224,13 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(reps):
-        g_main.replay()
-    if g_rem is not None:
-        g_rem.replay()
-    ev1.record(stream)
+    with torch.cuda.stream(stream):        # graph replays run on the current stream
+        ev0.record(stream)
+        for _ in range(reps):
+            g_main.replay()
+        if g_rem is not None:
+            g_rem.replay()
+        ev1.record(stream)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -247,11 +249,12 @@ def run_ours(args, rank, world, local_rank):
     with torch.cuda.graph(gw, stream=stream):
         for _ in range(256):
             plan0.spmv(xs[0], ys[0], stream=torch.cuda.current_stream())
-    gw.replay()
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    gw.replay()
-    ev1.record(stream)
+    with torch.cuda.stream(stream):
+        gw.replay()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        gw.replay()
+        ev1.record(stream)
     torch.cuda.synchronize()
     warm_ms = ev0.elapsed_time(ev1) / 256
 

@@ -162,6 +162,50 @@ void free_taichi(int num_shapes, TaiChi *t)
     free(t);
 }
 
+// TaiChi.cu:677-879: one shape box; the histogram, density test, hole rows
+// and claims run on the GPU, the result fills the reference's TaiChi record
+// (arrays malloc'd, released by free_taichi) and csrVal gets FLT_MAX marks.
+void partition_dia_shape(int M, int N, int nnz, int *&csrRow, int *&csrCol, float *&csrVal,
+                         float gain, shape &hi, TaiChi &t)
+{
+    (void)N; (void)gain;
+    t.M_sub = hi.b; t.N_sub = hi.a; t.xStart = hi.x; t.yStart = hi.y;
+    t.shape = 0;
+    tc::OneShape o;
+    tc_status st = tc::gpu_one_shape(M, nnz, csrRow, csrCol, csrVal, hi.x, hi.y, hi.a, hi.b, 0.6, o);
+    if (st != TC_OK) {
+        printf("CUDA Runtime Error: %s\n", tc_last_error());
+        t.neg = 0;
+        return;
+    }
+    t.width = o.width;
+    t.neg = o.neg;
+    if (o.neg <= 0) return;
+    auto dup = [](const std::vector<int> &v) {
+        int *p = (int *)malloc(std::max<size_t>(v.size(), 1) * sizeof(int));
+        if (!v.empty()) memcpy(p, v.data(), v.size() * sizeof(int));
+        return p;
+    };
+    t.neg_offsets = dup(o.offs);
+    t.start = dup(o.start);
+    t.end = dup(o.end);
+    t.numZeroNeg = dup(o.nzero);
+    t.cStart = (int *)malloc(sizeof(int) * o.neg);
+    int maxz = 0;
+    for (int d = 0; d < o.neg; ++d) {
+        t.cStart[d] = o.offs[d] > 0 ? o.offs[d] : 0;
+        maxz = std::max(maxz, o.nzero[d]);
+    }
+    t.nnz = (int)o.nnz;
+    t.maxNumZero = maxz;
+    t.rowZeroNeg = (int **)calloc(o.neg, sizeof(int *));
+    if (maxz > 0)
+        for (int d = 0; d < o.neg; ++d) {
+            t.rowZeroNeg[d] = (int *)malloc(sizeof(int) * maxz);
+            if (!o.holes[d].empty()) memcpy(t.rowZeroNeg[d], o.holes[d].data(), o.holes[d].size() * sizeof(int));
+        }
+}
+
 // TaiChi.cu:313-638: the partition runs on the GPU; the result is returned
 // in malloc'd host arrays exactly as the reference lays them out.
 void partition_shapes(char *sdf_name, int M, int N, int nnz, int *&csrRow, int *&csrCol,

@@ -135,4 +135,14 @@ struct PartitionOut {
 tc_status gpu_partition(int M, int N, int64_t nnz, const int *d_rowptr, const int *d_col,
                         const float *d_val, const tc_params &prm, bool keep_stages,
                         bool want_claimed, cudaStream_t s, PartitionOut &out);
+
+// Dense-diagonal extraction of one shape box on host arrays (marks h_val).
+struct OneShape {
+    int width = 0, neg = 0;
+    long nnz = 0;
+    std::vector<int> offs, start, end, nzero;
+    std::vector<std::vector<int>> holes;   // local hole rows per dense diagonal
+};
+tc_status gpu_one_shape(int M, int64_t nnz, const int *h_rowptr, const int *h_col, float *h_val,
+                        int x, int y, int a, int b, double density, OneShape &o);
 }  // namespace tc

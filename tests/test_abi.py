@@ -63,7 +63,7 @@ int main() {
                     os.path.join(d, "l.cpp"), "-o", exe], check=True)
     got = subprocess.run([exe], stdout=subprocess.PIPE, text=True, check=True).stdout.split()
     # 7 ints + pad, 7 pointers | char + 5 ints .. | 1 + 1024 + 10 ints
-    assert [int(v) for v in got] == [88, 32, 80, 104, 88, 1068]
+    assert [int(v) for v in got] == [88, 32, 80, 104, 80, 1068]
 
 
 def test_status_strings(tc):

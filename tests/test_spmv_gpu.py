@@ -126,13 +126,21 @@ def test_empty_and_tiny(tc, dev):
 
 
 def test_hybrid_without_csr_remainder(tc, dev):
-    """All non-zeros on hole-free dense diagonals: the reference leaves the CSR
-    unallocated and its kernel reads an invalid pointer; here y is exact."""
-    M, N, rp, col = matgen.segments(20000, [(0, 20000, 0, 1, 1.0)], noise=0, seed=1)
+    """All non-zeros on hole-free dense diagonals, so the CSR remainder is
+    empty: the reference leaves csrRow unallocated and its kernel reads an
+    invalid pointer (TaiChi.cu:579, 1362); here y is the diagonal sums."""
+    case = next(c for c in cases.MATRIX_CASES if c["name"] == "multi_shape")
+    M, N, rp, col = cases.matrix(case)
     fmt, _ = oracle.partition(M, N, rp, col)
-    assert fmt["dia_shapes"] == 1 and fmt["zero_elements"] + fmt["sparse_nnz"] == 0
-    plan = tc.Plan.from_format(M, N, fmt)
-    check_plan(plan, fmt, M, N, rp, col, dev, "no-remainder")
+    assert fmt["dia_shapes"] == 3
+    diag_only = dict(fmt, zero_elements=0, sparse_nnz=0, csrRow=np.zeros(M + 1, np.int32),
+                     csrCol=np.zeros(0, np.int32))
+    plan = tc.Plan.from_format(M, N, diag_only)
+    x = np.random.default_rng(4).integers(-8, 9, N).astype(np.float64)
+    y = run_spmv(plan, x, M, dev)
+    want = oracle.spmv_format_f64(diag_only, M, N, x)
+    assert np.abs(want).sum() > 0
+    np.testing.assert_array_equal(y.astype(np.float64), want)
 
 
 def test_spmv_host_e2e(tc, dev):
