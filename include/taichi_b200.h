@@ -51,14 +51,17 @@ typedef struct tc_params {
     int min_shape_side;   /* shapes with a smaller side are skipped (1000)     */
     double density;       /* a diagonal is dense if nnz/len >= density (0.6)   */
     int tile_rows;        /* max rows per multiply tile (1024)                 */
-    int tile_nnz;         /* max CSR entries per multiply tile (4096)          */
-    int vector_threshold; /* tiles whose longest row exceeds this use a warp
-                             per row instead of a thread per row (32)          */
+    int tile_nnz;         /* rows with more CSR entries get a CTA each (2048)  */
+    int max_lanes;        /* most lanes the planner gives one row: 1..32 (32)  */
+    int ctas_per_sm;      /* resident CTAs per SM of the multiply grid (4)     */
     int flags;            /* TC_FLAG_*                                         */
 } tc_params;
 
 #define TC_FLAG_NO_PARTITION 0x1  /* skip the morphology: plain CSR plan      */
 #define TC_FLAG_KEEP_HOST    0x2  /* keep a host copy of the format (export)  */
+#define TC_FLAG_NO_PDL       0x4  /* launch without programmatic dependent
+                                     launch (the multiply then starts only
+                                     when the previous kernel has finished)  */
 
 TC_API void tc_params_default(tc_params *p);
 
@@ -124,6 +127,10 @@ TC_API tc_status tc_plan_export(const tc_plan *plan, int *xStart, int *yStart, i
 TC_API tc_status tc_plan_thumbnail(const tc_plan *plan, unsigned char *stages, int *W,
                             int *corners, int *ncorners);
 
+/* TC_ERR_TIMEOUT if a multiply of this plan gave up a bounded device-side
+ * wait (its y is then incomplete); TC_OK otherwise.  Synchronous. */
+TC_API tc_status tc_plan_check(const tc_plan *plan);
+
 /* y = A x.  d_x: N floats, d_y: M floats, device memory.  Stream-ordered. */
 TC_API tc_status tc_spmv(const tc_plan *plan, const float *d_x, float *d_y, void *stream);
 
@@ -169,6 +176,28 @@ TC_API tc_status tc_read_mtx(const char *path, int *M, int *N, int64_t *nnz, int
 TC_API void tc_free(void *p);
 
 /* ----------------------------------------------------------------------- */
+/* Autotuner: density threshold and tile shape, timed per matrix.           */
+/* ----------------------------------------------------------------------- */
+typedef struct tc_tune_result {
+    tc_params params;       /* fastest parameters found                         */
+    double spmv_us;         /* their mean multiply time (back-to-back launches) */
+    double default_us;      /* the base parameters' time                        */
+    int trials;             /* candidates timed (0 when served from the cache)  */
+    int cached;             /* 1 when the result came from the cache            */
+    uint64_t fingerprint;   /* matrix fingerprint the result is cached under    */
+} tc_tune_result;
+
+/* Partitions the host CSR at several density thresholds and tries several
+ * tile shapes on the best format (at most max_trials candidates; <= 0 means
+ * 32), timing each on the GPU.  Results are cached per matrix fingerprint
+ * for the life of the process.  No counterpart in the reference, which fixes
+ * the threshold at 0.6 (TaiChi.cu:757). */
+TC_API tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const int *col,
+                         const tc_params *base, int max_trials, void *stream,
+                         tc_tune_result *out);
+TC_API void tc_tune_cache_clear(void);
+
+/* ----------------------------------------------------------------------- */
 /* Batched form: many resident plans in one persistent launch.              */
 /* ----------------------------------------------------------------------- */
 typedef struct tc_batch tc_batch;
@@ -180,6 +209,47 @@ TC_API tc_status tc_batch_create(int n, tc_plan *const *plans, const float *cons
 TC_API tc_status tc_batch_run(tc_batch *b, void *stream);              /* one launch  */
 TC_API tc_status tc_batch_graph_launch(tc_batch *b, void *stream);     /* graph replay */
 TC_API tc_status tc_batch_destroy(tc_batch *b);
+
+/* ----------------------------------------------------------------------- */
+/* Served form: resident matrices, admission by HBM footprint, continuous   */
+/* batching of SpMV requests.  No counterpart in the reference.             */
+/* ----------------------------------------------------------------------- */
+typedef struct tc_server tc_server;
+
+typedef struct tc_serve_config {
+    int64_t hbm_budget;   /* bytes for admitted plans + request arenas (64 GiB)    */
+    int64_t arena_bytes;  /* device x / y space of one launch context (256 MiB)   */
+    int contexts;         /* launch contexts (streams) in flight (3)             */
+    int max_batch;        /* most requests packed into one launch (64, <= 256)   */
+    int max_plans;        /* size of the resident plan table (1024)              */
+} tc_serve_config;
+
+typedef struct tc_serve_stats {
+    int64_t requests, batches;
+    double seconds;       /* first arrival to last completion                    */
+    double spmv_per_s;    /* requests / seconds                                  */
+    double p50_ms, p99_ms, mean_ms, max_ms;   /* completion - arrival            */
+    double mean_batch;    /* requests per launch                                 */
+} tc_serve_stats;
+
+TC_API void tc_serve_config_default(tc_serve_config *c);
+TC_API tc_status tc_server_create(const tc_serve_config *c, tc_server **out);
+/* Makes `plan` resident in the server (not owned; keep it alive).  Returns
+ * TC_ERR_CAPACITY when its HBM footprint does not fit the budget left, or its
+ * x and y do not fit an arena. */
+TC_API tc_status tc_server_admit(tc_server *s, tc_plan *plan, int *matrix_id);
+TC_API tc_status tc_server_evict(tc_server *s, int matrix_id);
+TC_API int64_t tc_server_hbm_used(const tc_server *s);
+/* Serves a request trace in real time: request r arrives arrival_s[r]
+ * seconds after the call starts (non-decreasing), multiplies matrix[r] by the
+ * host vector h_x[r] and leaves y in h_y[r] (pinned host memory gives full
+ * copy bandwidth).  mode 0: continuous batching; mode 1: one synchronous
+ * request at a time (the plain form).  latency_ms[r] (optional) receives
+ * completion minus arrival. */
+TC_API tc_status tc_server_run(tc_server *s, int nreq, const double *arrival_s, const int *matrix,
+                               const float *const *h_x, float *const *h_y, int mode,
+                               double *latency_ms, tc_serve_stats *stats);
+TC_API tc_status tc_server_destroy(tc_server *s);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,7 @@ _LIB = None
 
 TC_FLAG_NO_PARTITION = 0x1
 TC_FLAG_KEEP_HOST = 0x2
+TC_FLAG_NO_PDL = 0x4
 
 _IP = C.POINTER(C.c_int)
 
@@ -31,8 +32,8 @@ class TcError(RuntimeError):
 class Params(C.Structure):
     _fields_ = [("thumb_height", C.c_int), ("open_len", C.c_int), ("eye_size", C.c_int),
                 ("min_contour", C.c_int), ("min_shape_side", C.c_int), ("density", C.c_double),
-                ("tile_rows", C.c_int), ("tile_nnz", C.c_int), ("vector_threshold", C.c_int),
-                ("flags", C.c_int)]
+                ("tile_rows", C.c_int), ("tile_nnz", C.c_int), ("max_lanes", C.c_int),
+                ("ctas_per_sm", C.c_int), ("flags", C.c_int)]
 
 
 class Format(C.Structure):
@@ -55,10 +56,17 @@ class PlanInfo(C.Structure):
 EXPORTS = (
     "tc_params_default", "tc_last_error", "tc_status_string", "tc_plan_create",
     "tc_plan_from_format", "tc_plan_destroy", "tc_plan_info_get", "tc_plan_export",
-    "tc_plan_thumbnail", "tc_spmv", "tc_spmv_host", "tc_spmm", "tc_getsdf",
+    "tc_plan_thumbnail", "tc_plan_check", "tc_spmv", "tc_spmv_host", "tc_spmm", "tc_getsdf",
     "tc_trace_contours", "tc_read_mtx", "tc_free", "tc_batch_create", "tc_batch_run",
-    "tc_batch_graph_launch", "tc_batch_destroy",
+    "tc_batch_graph_launch", "tc_batch_destroy", "tc_tune", "tc_tune_cache_clear",
+    "tc_serve_config_default", "tc_server_create", "tc_server_admit", "tc_server_evict",
+    "tc_server_hbm_used", "tc_server_run", "tc_server_destroy",
 )
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("params", Params), ("spmv_us", C.c_double), ("default_us", C.c_double),
+                ("trials", C.c_int), ("cached", C.c_int), ("fingerprint", C.c_uint64)]
 
 
 def lib():
@@ -82,6 +90,7 @@ def lib():
         L.tc_plan_info_get.argtypes = [vp, C.POINTER(PlanInfo)]
         L.tc_plan_export.argtypes = [vp] + [vp] * 7
         L.tc_plan_thumbnail.argtypes = [vp, vp, _IP, vp, _IP]
+        L.tc_plan_check.argtypes = [vp]
         L.tc_spmv.argtypes = [vp, vp, vp, vp]
         L.tc_spmv_host.argtypes = [vp, vp, vp, vp]
         L.tc_spmm.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp]
@@ -95,6 +104,20 @@ def lib():
         L.tc_batch_run.argtypes = [vp, vp]
         L.tc_batch_graph_launch.argtypes = [vp, vp]
         L.tc_batch_destroy.argtypes = [vp]
+        L.tc_tune.argtypes = [C.c_int, C.c_int, C.c_int64, vp, vp, C.POINTER(Params), C.c_int, vp,
+                              C.POINTER(TuneResult)]
+        L.tc_tune_cache_clear.argtypes = []
+        L.tc_tune_cache_clear.restype = None
+        L.tc_serve_config_default.argtypes = [C.POINTER(ServeConfig)]
+        L.tc_serve_config_default.restype = None
+        L.tc_server_create.argtypes = [C.POINTER(ServeConfig), C.POINTER(vp)]
+        L.tc_server_admit.argtypes = [vp, vp, C.POINTER(C.c_int)]
+        L.tc_server_evict.argtypes = [vp, C.c_int]
+        L.tc_server_hbm_used.argtypes = [vp]
+        L.tc_server_hbm_used.restype = C.c_int64
+        L.tc_server_run.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp,
+                                    C.POINTER(ServeStats)]
+        L.tc_server_destroy.argtypes = [vp]
         _LIB = L
     return _LIB
 
@@ -133,6 +156,81 @@ def _stream(s):
     if isinstance(s, int):
         return s
     return s.cuda_stream
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_int64), ("arena_bytes", C.c_int64), ("contexts", C.c_int),
+                ("max_batch", C.c_int), ("max_plans", C.c_int)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("requests", C.c_int64), ("batches", C.c_int64), ("seconds", C.c_double),
+                ("spmv_per_s", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("mean_batch", C.c_double)]
+
+
+class Server:
+    """Resident matrices + continuous batching of SpMV requests (tc_server)."""
+
+    def __init__(self, **cfg):
+        L = lib()
+        c = ServeConfig()
+        L.tc_serve_config_default(C.byref(c))
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        self._h = C.c_void_p()
+        check(L.tc_server_create(C.byref(c), C.byref(self._h)))
+        self._plans = {}
+
+    def admit(self, plan):
+        i = C.c_int()
+        check(lib().tc_server_admit(self._h, plan.handle, C.byref(i)))
+        self._plans[i.value] = plan
+        return i.value
+
+    def evict(self, mid):
+        check(lib().tc_server_evict(self._h, mid))
+        self._plans.pop(mid, None)
+
+    def hbm_used(self):
+        return lib().tc_server_hbm_used(self._h)
+
+    def run(self, arrival_s, matrix, xs, ys, mode=0):
+        """xs / ys: per-request host arrays (numpy, float32, contiguous).
+        Returns (stats dict, latency_ms array)."""
+        n = len(matrix)
+        arr = np.ascontiguousarray(arrival_s, np.float64)
+        mat = np.ascontiguousarray(matrix, np.int32)
+        X = (C.c_void_p * n)(*[_ptr(a) for a in xs])
+        Y = (C.c_void_p * n)(*[_ptr(a) for a in ys])
+        lat = np.zeros(n, np.float64)
+        st = ServeStats()
+        check(lib().tc_server_run(self._h, n, arr.ctypes.data, mat.ctypes.data, X, Y, mode,
+                                  lat.ctypes.data, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}, lat
+
+    def close(self):
+        if self._h:
+            lib().tc_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tune(M, N, rowptr, col, prm=None, max_trials=32, stream=None):
+    """Autotunes the partition threshold and tile shape for a host CSR;
+    returns a TuneResult (params usable with Plan.from_csr)."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    r = TuneResult()
+    check(lib().tc_tune(M, N, int(rowptr[M]), rowptr.ctypes.data, col.ctypes.data,
+                        C.byref(prm) if prm is not None else None, max_trials, _stream(stream),
+                        C.byref(r)))
+    return r
 
 
 def read_mtx(path):
@@ -259,6 +357,10 @@ class Plan:
     # -- multiply -----------------------------------------------------------
     def spmv(self, x, y, stream=None):
         check(lib().tc_spmv(self._h, _ptr(x), _ptr(y), _stream(stream)))
+
+    def check(self):
+        """Raises if a multiply of this plan reported a device-side timeout."""
+        check(lib().tc_plan_check(self._h))
 
     def spmv_host(self, x, y, stream=None):
         check(lib().tc_spmv_host(self._h, _ptr(x), _ptr(y), _stream(stream)))

@@ -64,8 +64,9 @@ void tc_params_default(tc_params *p)
     p->min_shape_side = 1000;  // TaiChi.cu:379
     p->density = 0.6;          // TaiChi.cu:757
     p->tile_rows = 1024;
-    p->tile_nnz = 4096;
-    p->vector_threshold = 32;
+    p->tile_nnz = 2048;
+    p->max_lanes = 32;
+    p->ctas_per_sm = 4;
     p->flags = 0;
 }
 
@@ -77,8 +78,11 @@ static tc_status check_params(const tc_params &p)
         return fail(TC_ERR_INVALID, "morphology element sizes out of range");
     if (p.tile_rows < 1 || p.tile_rows > tc::kMaxTileRows)
         return fail(TC_ERR_INVALID, "tile_rows %d outside [1, %d]", p.tile_rows, tc::kMaxTileRows);
-    if (p.tile_nnz < 1 || p.tile_nnz > tc::kMaxTileNnz)
-        return fail(TC_ERR_INVALID, "tile_nnz %d outside [1, %d]", p.tile_nnz, tc::kMaxTileNnz);
+    if (p.tile_nnz < 1) return fail(TC_ERR_INVALID, "tile_nnz %d < 1", p.tile_nnz);
+    if (p.ctas_per_sm < 1 || p.ctas_per_sm > 32)
+        return fail(TC_ERR_INVALID, "ctas_per_sm %d outside [1, 32]", p.ctas_per_sm);
+    if (p.max_lanes < 1 || p.max_lanes > 32 || (p.max_lanes & (p.max_lanes - 1)))
+        return fail(TC_ERR_INVALID, "max_lanes %d is not a power of two in [1, 32]", p.max_lanes);
     return TC_OK;
 }
 
@@ -203,6 +207,14 @@ tc_status tc_plan_thumbnail(const tc_plan *p, unsigned char *stages, int *W, int
     return TC_OK;
 }
 
+tc_status tc_plan_check(const tc_plan *p)
+{
+    if (!p) return fail(TC_ERR_INVALID, "null plan");
+    int e = 0;
+    TC_CUDA(cudaMemcpy(&e, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    return e ? fail(TC_ERR_TIMEOUT, "a multiply of this plan gave up waiting for its staged tiles") : TC_OK;
+}
+
 tc_status tc_spmv(const tc_plan *p, const float *d_x, float *d_y, void *stream)
 {
     if (!p || (!d_x && p->N) || (!d_y && p->M)) return fail(TC_ERR_INVALID, "tc_spmv: null argument");
@@ -223,7 +235,7 @@ tc_status tc_spmv_host(const tc_plan *cp, const float *h_x, float *h_y, void *st
     TC_CHECK(tc::launch_spmv(p->dev_plan(), p->d_xbuf, p->d_ybuf, s));
     if (p->M) TC_CUDA(cudaMemcpyAsync(h_y, p->d_ybuf, sizeof(float) * (size_t)p->M, cudaMemcpyDeviceToHost, s));
     TC_CUDA(cudaStreamSynchronize(s));
-    return TC_OK;
+    return tc_plan_check(p);
 }
 
 tc_status tc_spmm(const tc_plan *p, const float *d_X, int ldx, int k, float *d_Y, int ldy, void *stream)

@@ -1,7 +1,7 @@
 // tc_batch.cu -- many resident plans multiplied in one persistent launch.
 //
 // The batch flattens the tile lists of all its plans into one work list of
-// (plan, tile) pairs, longest tiles first, and launches one grid of
+// (plan, tile) pairs in plan order and launches one grid of
 // (SMs x resident CTAs) CTAs that stride over it.  Every tile runs the same
 // device code as the single-plan kernel, so each matrix's y is bit-identical
 // alone and inside a batch.  The launch can be captured once in a CUDA graph
@@ -29,16 +29,14 @@ __global__ void __launch_bounds__(kBlock) batch_kernel(const DevPlan *__restrict
                                                        int nitems, const float *const *xs,
                                                        float *const *ys)
 {
-    extern __shared__ __align__(16) char smem[];
     for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
         const BatchItem it = items[w];
-        const DevPlan p = plans[it.plan];
+        const DevPlan &p = plans[it.plan];     // read in place (global memory)
         const Tile t = p.tiles[it.tile];
         const float *x = xs[it.plan];
         float *y = ys[it.plan];
-        if (p.hybrid) run_tile<true>(p, t, x, y, smem);
-        else run_tile<false>(p, t, x, y, smem);
-        __syncthreads();
+        if (p.hybrid) run_tile<true>(p, t, x, y);
+        else run_tile<false>(p, t, x, y);
     }
 }
 
@@ -70,26 +68,16 @@ tc_status tc_batch_create(int n, tc_plan *const *plans, const float *const *d_x,
     *out = nullptr;
     std::vector<tc::DevPlan> dps(n);
     std::vector<tc::BatchItem> items;
-    std::vector<int64_t> cost;
-    int rows_cap = 1, nnz_cap = 1, span = 0;
     for (int i = 0; i < n; ++i) {
         if (!plans[i]) return fail(TC_ERR_INVALID, "plan %d is null", i);
         dps[i] = plans[i]->dev_plan();
-        rows_cap = std::max(rows_cap, dps[i].rows_cap);
-        nnz_cap = std::max(nnz_cap, dps[i].nnz_cap);
-        span = std::max(span, dps[i].max_span);
         for (int t = 0; t < dps[i].ntiles; ++t) items.push_back(tc::BatchItem{i, t});
-    }
-    // every tile uses the largest caps' shared-memory layout
-    for (int i = 0; i < n; ++i) {
-        dps[i].rows_cap = rows_cap;
-        dps[i].nnz_cap = nnz_cap;
     }
     tc_batch *b = new (std::nothrow) tc_batch();
     if (!b) return fail(TC_ERR_ALLOC, "host allocation");
     b->n = n;
     b->nitems = (int)items.size();
-    b->smem = tc::spmv_smem_bytes(rows_cap, nnz_cap, span);
+    b->smem = 0;
     size_t o_pl = 0;
     size_t o_it = (sizeof(tc::DevPlan) * n + 255) & ~(size_t)255;
     size_t o_x = o_it + ((sizeof(tc::BatchItem) * items.size() + 255) & ~(size_t)255);
@@ -107,8 +95,6 @@ tc_status tc_batch_create(int n, tc_plan *const *plans, const float *const *d_x,
         e = cudaMemcpy(b->d_items, items.data(), sizeof(tc::BatchItem) * items.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_x, d_x, sizeof(void *) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_y, d_y, sizeof(void *) * n, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(tc::batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
     int per_sm = 0, dev = 0, sms = 0;
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::batch_kernel, tc::kBlock, b->smem);

@@ -31,11 +31,12 @@ tc_status fail(tc_status s, const char *fmt, ...);
     } while (0)
 
 // ------------------------------------------------------------- tile plan
-// A multiply tile is a run of consecutive rows processed by one CTA.
+// A multiply tile is a run of consecutive rows processed by one CTA.  Kinds
+// TILE_L1..TILE_L32 give 1..32 lanes to each row; TILE_LONG gives one row a
+// whole CTA.
 enum TileKind : int {
-    TILE_SCALAR = 0,   // thread per row, CSR entries staged in shared memory
-    TILE_VECTOR = 1,   // warp per row, CSR entries staged in shared memory
-    TILE_LONG = 2      // one long row, CTA-wide reduction straight from HBM
+    TILE_L1 = 0, TILE_L2 = 1, TILE_L4 = 2, TILE_L8 = 3, TILE_L16 = 4, TILE_L32 = 5,
+    TILE_LONG = 6
 };
 
 struct Tile {          // 16 bytes, read once per CTA
@@ -48,10 +49,9 @@ struct Tile {          // 16 bytes, read once per CTA
 __host__ __device__ inline int tile_nrows(const Tile &t) { return t.nrows_kind & 0x0fffffff; }
 __host__ __device__ inline int tile_kind(const Tile &t) { return (t.nrows_kind >> 28) & 0xf; }
 
-// Compile-time limits of the tile kernel (shared-memory staging buffers).
-constexpr int kBlock = 256;           // threads per CTA
-constexpr int kMaxTileRows = 2040;    // rows staged per tile (rows+1 <= 8*kBlock)
-constexpr int kMaxTileNnz = 8192;     // CSR entries staged per tile
+constexpr int kBlock = 256;           // threads per CTA of the multiply kernels
+constexpr int kMaxTileRows = 1 << 20; // planner limit on rows per tile
+constexpr int kStageNnz = 8192;       // CSR words of a tile staged in shared memory
 
 // Everything a multiply kernel needs about one plan (passed by value).
 struct DevPlan {
@@ -63,7 +63,10 @@ struct DevPlan {
     const int *offsets;     // num_negs
     int M, N, ntiles, dia_shapes, row_start, row_stop, hybrid;
     int max_span;           // widest offset span of any shape (max-min)
-    int rows_cap, nnz_cap;  // tile limits the plan was built with
+    int pdl;                // launch with programmatic stream serialization
+    int stage_rp, stage_cw; // ints per shared-memory stage (row pointers, CSR words)
+    int grid;               // persistent grid size
+    int *err;               // device error word (1: a bounded wait gave up)
 };
 
 struct tc_plan_impl;
@@ -88,6 +91,8 @@ struct tc_plan {
     int2 *d_shape_dias = nullptr;
     int ntiles = 0, ntiles_vector = 0, ntiles_long = 0;
     int max_span = 0;
+    int stage_rp = 8, stage_cw = 8, grid = 1;
+    int *d_err = nullptr;
     // host copies of the small format arrays (always) and optionally the CSR
     std::vector<int> h_xStart, h_yStart, h_xStop, h_nDiasPtr, h_offsets;
     std::vector<int> h_rowptr, h_cols;   // only with TC_FLAG_KEEP_HOST
@@ -115,7 +120,6 @@ void plan_tiles(const int *rowptr, int M, const tc_params &prm, std::vector<Tile
 tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
 tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,
                       cudaStream_t s);
-size_t spmv_smem_bytes(int rows_cap, int nnz_cap, int max_span);
 
 // GPU partitioner: device CSR in, format (host vectors) out.
 struct PartitionOut {

@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(1024) morph_kernel(MorphArgs a)
     // D = B - O2 (saturating) -> T1
     for (int i = threadIdx.x; i < n; i += blockDim.x) T1.w[i] = B.w[i] & ~O2w.w[i];
     __syncthreads();
-    if (a.use_smem) for (int i = threadIdx.x; i < n; i += blockDim.x) D.w[i] = T1.w[i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) D.w[i] = T1.w[i];
     // E = open eye(5) (D)
     Img Ew = a.use_smem ? T3 : E;
     erode_dilate_eye(T1, T2, Ew, a.eye);
@@ -654,6 +654,20 @@ __global__ void sparse_scatter(const int *__restrict__ rowptr, const int *__rest
 
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 
+// Input check: rowptr[0] == 0, non-decreasing, rowptr[M] == nnz, 0 <= col < N.
+__global__ void validate_csr(const int *__restrict__ rowptr, const int *__restrict__ col, int M,
+                             int N, long nnz, int *__restrict__ bad)
+{
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < M; r += stride)
+        if (rowptr[r + 1] < rowptr[r]) atomicOr(bad, 1);
+    for (long j = (long)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += stride) {
+        const int c = col[j];
+        if (c < 0 || c >= N) atomicOr(bad, 2);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (rowptr[0] != 0 || rowptr[M] != nnz)) atomicOr(bad, 4);
+}
+
 int band_width(int s)     // TaiChi.cu:689-699
 {
     double w;
@@ -960,9 +974,18 @@ tc_status gpu_partition(int M, int N, int64_t nnz, const int *d_rowptr, const in
     auto t0 = std::chrono::steady_clock::now();
     out = PartitionOut();
     if (M < 0 || N < 0 || nnz < 0) return fail(TC_ERR_INVALID, "negative sizes");
-    DevBuf claim;
+    DevBuf claim, bad;
     TC_CHECK(claim.alloc((size_t)std::max<int64_t>(nnz, 1)));
+    TC_CHECK(bad.alloc(sizeof(int)));
     const int T = 256;
+    TC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    validate_csr<<<std::max(1, std::min(cdiv(std::max<long>(nnz, M), T), sm_count() * 16)), T, 0, s>>>(
+        d_rowptr, d_col, M, N, nnz, bad.as<int>());
+    int hbad = 0;
+    TC_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TC_CUDA(cudaStreamSynchronize(s));
+    if (hbad) return fail(TC_ERR_FORMAT, "invalid CSR input (code %d: 1 rowptr decreases, 2 column "
+                                         "outside [0, N), 4 rowptr[0]/rowptr[M] wrong)", hbad);
     if (nnz) claim_init<<<cdiv(nnz, T), T, 0, s>>>(d_val, claim.as<unsigned char>(), nnz);
     TC_CUDA(cudaGetLastError());
 

@@ -1,18 +1,16 @@
-// tc_spmv.cu -- the multiply: tile planner, device format upload and the
+// tc_spmv.cu -- the multiply: tile planner, device format upload, and the
 // value-free hybrid SpMV / SpMM kernels for sm_100a.
 //
-// Replaces taichi_SpMV's dispatch and kernels (TaiChi.cu:965-1329): the
-// reference picks one of four CSR-vector kernels with a fixed vector width per
-// matrix; here one kernel walks a precomputed list of row tiles whose kind
-// (thread per row / warp per row / CTA per long row) was chosen from the
-// row-length histogram, stages each tile's row pointers and CSR entries in
-// shared memory with batched coalesced loads, streams the x window of every
-// dense diagonal through shared memory with 16-byte loads, and writes y once
-// (the diagonal and CSR parts are merged in registers).
-//
-// Arithmetic (per row, FP32): the signed CSR entries in stored order (holes
-// subtract, leftovers add), then the dense diagonals shape by shape in offset
-// order -- the same terms as TaiChi.cu:1007-1024.
+// Replaces taichi_SpMV's dispatch and kernels (TaiChi.cu:965-1329).  The
+// reference launches one of four CSR-vector kernels with a single vector
+// width per matrix (TPV = sqrt of the mean row length) and a volatile
+// shared-memory reduction.  Here the host planner cuts the rows into tiles
+// and gives each tile its own lanes-per-row from that tile's row lengths (a
+// CTA per row above a length limit); the kernel walks the tile list, keeps
+// kRPT rows' loads in flight per lane group, adds the dense-diagonal terms in
+// registers and writes y once with warp-shuffle reductions.  Launches use
+// programmatic dependent launch so the next multiply's index loads overlap
+// the previous one's tail.
 
 #include <cuda_runtime.h>
 
@@ -25,59 +23,208 @@
 namespace tc {
 
 // ------------------------------------------------------------------ planner
+// Lanes per row from the mean row length of a run of rows: one lane per row
+// until rows average more than 16 entries, then the smallest power of two
+// giving each lane about 8 entries, capped at max_lanes.  (The CSR words come
+// from shared memory, so a thread walking its own row costs no coalescing.)
+static int lanes_for(double mean, int max_lanes)
+{
+    if (mean <= 16.0) return 1;
+    int l = 1;
+    while (l < max_lanes && 8.0 * l < mean) l <<= 1;
+    return l;
+}
+
+static int kind_of(int lanes)
+{
+    int k = 0;
+    while ((1 << k) < lanes) ++k;
+    return k;
+}
+
 void plan_tiles(const int *rp, int M, const tc_params &prm, std::vector<Tile> &tiles, int *nvec,
                 int *nlong)
 {
+    const int long_len = std::max(1, std::min(prm.tile_nnz, kStageNnz));
     const int rows_cap = std::max(1, std::min(prm.tile_rows, kMaxTileRows));
-    const int nnz_cap = std::max(1, std::min(prm.tile_nnz, kMaxTileNnz));
-    const int vthr = prm.vector_threshold;
     tiles.clear();
     *nvec = *nlong = 0;
     int r = 0;
     while (r < M) {
-        int len = rp[r + 1] - rp[r];
-        if (len > nnz_cap) {
-            tiles.push_back(Tile{r, rp[r], len, 1 | (TILE_LONG << 28)});
+        if (rp[r + 1] - rp[r] > long_len) {
+            tiles.push_back(Tile{r, rp[r], rp[r + 1] - rp[r], 1 | (TILE_LONG << 28)});
             ++*nlong;
             ++r;
             continue;
         }
-        int start = r, nnz = 0, maxlen = 0;
-        while (r < M && r - start < rows_cap) {
-            len = rp[r + 1] - rp[r];
-            if (len > nnz_cap || nnz + len > nnz_cap) break;
-            nnz += len;
-            maxlen = std::max(maxlen, len);
-            ++r;
-        }
-        int kind = maxlen > vthr ? TILE_VECTOR : TILE_SCALAR;
-        *nvec += kind == TILE_VECTOR;
-        tiles.push_back(Tile{start, rp[start], nnz, (r - start) | (kind << 28)});
+        // candidate run: up to 1024 rows, stopping before a long row
+        int n = 0;
+        while (r + n < M && n < 1024 && rp[r + n + 1] - rp[r + n] <= long_len) ++n;
+        int lanes = lanes_for((double)(rp[r + n] - rp[r]) / n, prm.max_lanes);
+        int rows = std::min(std::min(n, tile_rows_for(lanes)), rows_cap);
+        while (rows > 1 && rp[r + rows] - rp[r] > kStageNnz) rows = (rows + 1) / 2;   // fits a stage
+        lanes = lanes_for((double)(rp[r + rows] - rp[r]) / rows, prm.max_lanes);
+        if (lanes > 1) ++*nvec;
+        tiles.push_back(Tile{r, rp[r], rp[r + rows] - rp[r], rows | (kind_of(lanes) << 28)});
+        r += rows;
     }
-}
-
-size_t spmv_smem_bytes(int rows_cap, int nnz_cap, int max_span)
-{
-    return spmv_smem_bytes_impl(rows_cap, nnz_cap, max_span);
 }
 
 // ------------------------------------------------------------------ kernels
 namespace {
 
+// ---- TMA bulk copies into shared memory, completion on an mbarrier ----
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *m, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)),
+                 "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *m)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *m, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_u32(m)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~1 s of polling (the copies complete in
+// microseconds; a give-up is reported through the plan's error word).
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, unsigned parity)
+{
+    for (long i = 0; i < (1L << 22); ++i)
+        if (mbar_test(m, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 16-byte aligned byte window [a, b) that covers elements [e0, e1) of an
+// int array (the plan arrays are padded, so the window stays inside them).
+struct Window {
+    long a, b;
+    int shift;   // index of element e0 inside the window
+};
+__device__ __forceinline__ Window window_of(long e0, long e1)
+{
+    Window w;
+    w.a = (e0 * 4) & ~15L;
+    w.b = (e1 * 4 + 15) & ~15L;
+    w.shift = (int)((e0 * 4 - w.a) >> 2);
+    return w;
+}
+
+// Issues the copies of tile t into stage s (thread 0 only).
+__device__ __forceinline__ void stage_tile(const DevPlan &p, int t, int *rp_buf, int *cw_buf,
+                                           uint64_t *bar)
+{
+    if (t >= p.ntiles) return;
+    const Tile tile = p.tiles[t];
+    if (tile_kind(tile) == TILE_LONG) return;
+    const Window wr = window_of(tile.row0, (long)tile.row0 + tile_nrows(tile) + 1);
+    const Window wc = window_of(tile.nz0, (long)tile.nz0 + tile.nnz);
+    const unsigned br = (unsigned)(wr.b - wr.a), bc = tile.nnz ? (unsigned)(wc.b - wc.a) : 0u;
+    mbar_expect_tx(bar, br + bc);
+    bulk_load(rp_buf, reinterpret_cast<const char *>(p.rowptr) + wr.a, br, bar);
+    if (bc) bulk_load(cw_buf, reinterpret_cast<const char *>(p.cols) + wc.a, bc, bar);
+}
+
+// The multiply: a persistent grid; each CTA walks tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ... with a two-stage pipeline: while one tile is
+// processed from shared memory, the TMA engine brings in the row pointers
+// and CSR words of the tile after next.  Rows longer than a stage are read
+// straight from global memory (TILE_LONG).
 template <bool SIGNED>
 __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const float *__restrict__ x,
                                                             float *__restrict__ y)
 {
-    extern __shared__ __align__(16) char smem[];
-    for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    int *const buf = reinterpret_cast<int *>(smem + 16);
+    const int stride = p.stage_rp + p.stage_cw;          // ints per stage
+    allow_next_grid();
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        stage_tile(p, blockIdx.x, buf, buf + p.stage_rp, bar);
+        stage_tile(p, blockIdx.x + gridDim.x, buf + stride, buf + stride + p.stage_rp, bar + 1);
+    }
+    unsigned phases = 0u;                                // bit s: parity of stage s
+    bool waited = false;
+    int i = 0;
+    for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        int *const rp_s = buf + s * stride;
+        int *const cw_s = rp_s + p.stage_rp;
         const Tile tile = p.tiles[t];
-        run_tile<SIGNED>(p, tile, x, y, smem);
-        __syncthreads();
+        if (tile_kind(tile) == TILE_LONG) {
+            run_tile<SIGNED>(p, tile, x, y, !waited);
+        } else {
+            const bool ok = mbar_wait(bar + s, (phases >> s) & 1u);
+            if (!__syncthreads_and(ok)) {          // every thread takes the same branch
+                if (threadIdx.x == 0) atomicExch(p.err, 1);
+                mbar_wait(bar + (s ^ 1), (phases >> (s ^ 1)) & 1u);   // copies in flight land
+                return;
+            }
+            phases ^= 1u << s;
+            const Window wr = window_of(tile.row0, 0), wc = window_of(tile.nz0, 0);
+            const SharedSrc src{rp_s + wr.shift, cw_s + wc.shift, tile.nz0};
+            run_tile_src<SIGNED>(p, tile, src, x, y, !waited);
+        }
+        waited = true;
+        __syncthreads();                  // stage s is free again
+        if (threadIdx.x == 0) {
+            fence_async_shared();
+            stage_tile(p, t + 2 * gridDim.x, rp_s, cw_s, bar + s);
+        }
+    }
+    if (!waited) wait_prior_grid();
+}
+
+// SpMM: a warp owns kRPW consecutive rows at a time; lane l holds columns
+// [l*V, l*V+V) of the k right-hand sides, so every X / Y row access is one
+// coalesced warp transaction.  The entries of the kRPW rows are walked in
+// rounds (one entry per row per round) so their X-row loads overlap.
+constexpr int kRPW = 4;
+
+template <int V>
+__device__ __forceinline__ void axpy_row(float (&acc)[V], const float *__restrict__ X, long off,
+                                         int c0, int k, float sg)
+{
+    const float *xr = X + off + c0;
+    if (V == 2 && c0 + 1 < k && ((reinterpret_cast<uintptr_t>(xr) & 7) == 0)) {
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(xr));
+        acc[0] += sg * v.x;
+        acc[V - 1] += sg * v.y;
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if (c0 + v < k) acc[v] += sg * __ldg(xr + v);
     }
 }
 
-// SpMM: one warp per row, lane l owns columns [l*V, l*V+V) of the k
-// right-hand sides.
 template <bool SIGNED, int V>
 __global__ void __launch_bounds__(kBlock) spmm_rows_kernel(DevPlan p, const float *__restrict__ X,
                                                            int ldx, int k, float *__restrict__ Y,
@@ -88,48 +235,71 @@ __global__ void __launch_bounds__(kBlock) spmm_rows_kernel(DevPlan p, const floa
     const int nwarps = (gridDim.x * kBlock) >> 5;
     const int c0 = lane * V;
     const bool active = c0 < k;
-    for (int r = warp; r < p.M; r += nwarps) {
-        float acc[V];
+    for (long r0l = (long)warp * kRPW; r0l < p.M; r0l += (long)nwarps * kRPW) {
+        const int r0 = (int)r0l;
+        // row pointers of the kRPW rows: lanes 0..nrow hold rowptr[r0 + lane]
+        const int nrow = min(kRPW, p.M - r0);
+        const int rpv = lane <= nrow ? __ldg(p.rowptr + r0 + lane) : 0;
+        int rb[kRPW], re[kRPW];
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = 0.f;
-        const int b = __ldg(p.rowptr + r), e = __ldg(p.rowptr + r + 1);
-        for (int j0 = b; j0 < e; j0 += 32) {
-            const int cnt = min(32, e - j0);
-            const int mine = lane < cnt ? __ldg(p.cols + j0 + lane) : 0;
-            for (int q = 0; q < cnt; ++q) {
-                const int cv = __shfl_sync(0xffffffffu, mine, q);
-                const int col = SIGNED ? (cv >> 1) : cv;
-                const float sg = (!SIGNED || (cv & 1)) ? 1.f : -1.f;
-                if (active) {
-                    const float *xr = X + (size_t)col * ldx + c0;
+        for (int q = 0; q < kRPW; ++q) {
+            rb[q] = __shfl_sync(0xffffffffu, rpv, q);
+            const int e = __shfl_sync(0xffffffffu, rpv, q + 1);
+            re[q] = q < nrow ? e : rb[q];
+        }
+        float acc[kRPW][V];
 #pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        if (c0 + v < k) acc[v] += sg * __ldg(xr + v);
-                }
+        for (int q = 0; q < kRPW; ++q)
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[q][v] = 0.f;
+        for (int t = 0;; ++t) {
+            bool any = false;
+            int cv[kRPW];
+#pragma unroll
+            for (int q = 0; q < kRPW; ++q) {
+                const int j = rb[q] + t;
+                cv[q] = j < re[q] ? __ldg(p.cols + j) : -1;
+                any |= cv[q] >= 0;
+            }
+            if (!any) break;            // uniform: every lane sees the same rows
+#pragma unroll
+            for (int q = 0; q < kRPW; ++q) {
+                if (cv[q] < 0 || !active) continue;
+                const int col = SIGNED ? (cv[q] >> 1) : cv[q];
+                const float sg = (!SIGNED || (cv[q] & 1)) ? 1.f : -1.f;
+                axpy_row<V>(acc[q], X, (long)col * ldx, c0, k, sg);
             }
         }
-        if (p.dia_shapes > 0 && r >= p.row_start && r < p.row_stop) {
-            for (int s = 0; s < p.dia_shapes; ++s) {
-                const int4 sh = __ldg(p.shapes + s);
-                if (r < sh.x || r >= sh.y) continue;
-                const int2 dr = __ldg(p.shape_dias + s);
-                for (int n = dr.x; n < dr.y; ++n) {
-                    const int col = r - sh.x + sh.z + __ldg(p.offsets + n);
-                    if (col < sh.z || col >= sh.z + sh.w) continue;
-                    if (active) {
-                        const float *xr = X + (size_t)col * ldx + c0;
+        if (p.dia_shapes > 0) {
 #pragma unroll
-                        for (int v = 0; v < V; ++v)
-                            if (c0 + v < k) acc[v] += __ldg(xr + v);
+            for (int q = 0; q < kRPW; ++q) {
+                const int r = r0 + q;
+                if (q >= nrow || r < p.row_start || r >= p.row_stop || !active) continue;
+                for (int s = 0; s < p.dia_shapes; ++s) {
+                    const int4 sh = __ldg(p.shapes + s);
+                    if (r < sh.x || r >= sh.y) continue;
+                    const int2 dr = __ldg(p.shape_dias + s);
+                    for (int n = dr.x; n < dr.y; ++n) {
+                        const int col = r - sh.x + sh.z + __ldg(p.offsets + n);
+                        if (col >= sh.z && col < sh.z + sh.w)
+                            axpy_row<V>(acc[q], X, (long)col * ldx, c0, k, 1.f);
                     }
                 }
             }
         }
         if (active) {
-            float *yr = Y + (size_t)r * ldy + c0;
 #pragma unroll
-            for (int v = 0; v < V; ++v)
-                if (c0 + v < k) yr[v] = acc[v];
+            for (int q = 0; q < kRPW; ++q) {
+                if (q >= nrow) continue;
+                float *yr = Y + (long)(r0 + q) * ldy + c0;
+                if (V == 2 && c0 + 1 < k && ((reinterpret_cast<uintptr_t>(yr) & 7) == 0)) {
+                    *reinterpret_cast<float2 *>(yr) = make_float2(acc[q][0], acc[q][V - 1]);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+                        if (c0 + v < k) yr[v] = acc[q][v];
+                }
+            }
         }
     }
 }
@@ -149,11 +319,16 @@ int num_sms()
 
 }  // namespace
 
+size_t stream_smem_bytes(const DevPlan &dp)
+{
+    return 16 + 2 * sizeof(int) * (size_t)(dp.stage_rp + dp.stage_cw);
+}
+
 template <bool SIGNED>
 static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaStream_t s)
 {
-    const size_t smem = spmv_smem_bytes(dp.rows_cap, dp.nnz_cap, dp.max_span);
-    // Opt-in above 48 KB of dynamic shared memory, once per device and size.
+    if (dp.ntiles <= 0) return TC_OK;
+    const size_t smem = stream_smem_bytes(dp);
     static size_t configured[2][64] = {};
     int dev = 0;
     TC_CUDA(cudaGetDevice(&dev));
@@ -163,10 +338,17 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured[SIGNED][dev] = smem;
     }
-    int grid = dp.ntiles;
-    if (grid <= 0) return TC_OK;
-    spmv_tiles_kernel<SIGNED><<<grid, kBlock, smem, s>>>(dp, x, y);
-    TC_CUDA(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(dp.grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = dp.pdl ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_tiles_kernel<SIGNED>, dp, x, y));
     return TC_OK;
 }
 
@@ -180,8 +362,8 @@ tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *
                       cudaStream_t s)
 {
     if (dp.M == 0) return TC_OK;
-    const int warps_needed = dp.M;
-    int grid = std::min((warps_needed + kBlock / 32 - 1) / (kBlock / 32), num_sms() * 8);
+    const long warps = (dp.M + kRPW - 1) / kRPW;
+    const int grid = (int)std::min<long>((warps + kBlock / 32 - 1) / (kBlock / 32), num_sms() * 16L);
     if (k <= 32) {
         if (dp.hybrid) spmm_rows_kernel<true, 1><<<grid, kBlock, 0, s>>>(dp, X, ldx, k, Y, ldy);
         else spmm_rows_kernel<false, 1><<<grid, kBlock, 0, s>>>(dp, X, ldx, k, Y, ldy);
@@ -213,8 +395,11 @@ tc::DevPlan tc_plan::dev_plan() const
     d.row_stop = row_stop;
     d.hybrid = hybrid;
     d.max_span = max_span;
-    d.rows_cap = std::max(1, std::min(params.tile_rows, tc::kMaxTileRows));
-    d.nnz_cap = std::max(1, std::min(params.tile_nnz, tc::kMaxTileNnz));
+    d.pdl = (params.flags & TC_FLAG_NO_PDL) ? 0 : 1;
+    d.stage_rp = stage_rp;
+    d.stage_cw = stage_cw;
+    d.grid = grid;
+    d.err = d_err;
     return d;
 }
 
@@ -237,6 +422,15 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     plan_tiles(csrRow, M, p->params, tiles, &p->ntiles_vector, &p->ntiles_long);
     p->ntiles = (int)tiles.size();
     p->nnz_csr = csrRow[M];
+    // shared-memory stage sizes (ints, multiples of 4) from the largest tile
+    int max_rows = 1, max_nnz = 0;
+    for (const Tile &t : tiles)
+        if (tile_kind(t) != TILE_LONG) {
+            max_rows = std::max(max_rows, tile_nrows(t));
+            max_nnz = std::max(max_nnz, t.nnz);
+        }
+    p->stage_rp = (max_rows + 1 + 8 + 3) & ~3;
+    p->stage_cw = (max_nnz + 8 + 3) & ~3;
 
     // shape table {xStart, xStop, yStart, Msub} and offset ranges
     std::vector<int4> shapes(p->dia_shapes);
@@ -252,7 +446,6 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
                 return fail(TC_ERR_FORMAT, "offsets of shape %d are not increasing", s);
         p->max_span = std::max(p->max_span, p->h_offsets[sd[s].y - 1] - p->h_offsets[sd[s].x]);
     }
-    if (p->max_span > 8192) return fail(TC_ERR_UNSUPPORTED, "diagonal span %d too wide", p->max_span);
 
     size_t o_rp = 0;
     size_t o_cols = align256(o_rp + sizeof(int) * ((size_t)M + 1) + 16);
@@ -260,7 +453,8 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     size_t o_sh = align256(o_tiles + sizeof(Tile) * tiles.size());
     size_t o_sd = align256(o_sh + sizeof(int4) * shapes.size());
     size_t o_off = align256(o_sd + sizeof(int2) * sd.size());
-    size_t total = align256(o_off + sizeof(int) * (size_t)p->num_negs + 16);
+    size_t o_err = align256(o_off + sizeof(int) * (size_t)p->num_negs + 16);
+    size_t total = align256(o_err + 16);
     char *base = nullptr;
     cudaError_t e = cudaMalloc(&base, total);
     if (e != cudaSuccess)
@@ -273,6 +467,19 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     p->d_shapes = reinterpret_cast<int4 *>(base + o_sh);
     p->d_shape_dias = reinterpret_cast<int2 *>(base + o_sd);
     p->d_offsets = reinterpret_cast<int *>(base + o_off);
+    p->d_err = reinterpret_cast<int *>(base + o_err);
+    {   // persistent grid: CTAs per SM from occupancy at this stage size
+        DevPlan tmp = p->dev_plan();
+        const size_t smem = stream_smem_bytes(tmp);
+        int per_sm = 0;
+        if (smem > 48 * 1024) {
+            TC_CUDA(cudaFuncSetAttribute(spmv_tiles_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            TC_CUDA(cudaFuncSetAttribute(spmv_tiles_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_tiles_kernel<true>, kBlock, smem));
+        const int cps = std::max(1, std::min(per_sm, p->params.ctas_per_sm));
+        p->grid = std::max(1, std::min(p->ntiles, cps * num_sms()));
+    }
     TC_CUDA(cudaMemsetAsync(base, 0, total, stream));
     TC_CUDA(cudaMemcpyAsync(p->d_rowptr, csrRow, sizeof(int) * ((size_t)M + 1),
                             cudaMemcpyHostToDevice, stream));

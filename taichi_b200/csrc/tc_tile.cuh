@@ -1,6 +1,20 @@
-// tc_tile.cuh -- device code of one multiply tile, shared by the single-plan
-// kernel (tc_spmv.cu) and the multi-plan persistent kernel (tc_batch.cu) so
-// that a matrix gets bit-identical y alone and inside a batch.
+// tc_tile.cuh -- device code of one multiply tile, shared by every multiply
+// kernel (single plan, batch, served) so that a matrix gets bit-identical y
+// whichever kernel runs it.
+//
+// A tile is a run of rows.  Its kind, chosen by the host planner from the
+// tile's row lengths, fixes how many lanes share a row (1, 2, 4, ..., 32); a
+// row longer than the planner's limit gets a whole CTA (TILE_LONG).  A lane
+// group handles kRPT rows per pass and keeps their loads in flight together.
+// Per row (FP32), each lane accumulates: the dense-diagonal terms of the
+// offsets it owns (offset order), then its CSR entries in stored order (holes
+// subtract, leftovers add); a butterfly reduction over the row's lanes ends
+// it.  These are the terms of TaiChi.cu:1007-1040 in a fixed order.
+//
+// The row pointers and CSR words of a tile come either straight from global
+// memory (GlobalSrc) or from a shared-memory copy that the TMA pipeline of the
+// multiply kernel brought in ahead of time (SharedSrc); the arithmetic is the
+// same for both.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,37 +25,25 @@
 
 namespace tc {
 
-// Shared memory of the tile kernel: row pointers, per-row sums, and one
-// buffer that first holds the tile's gathered CSR terms and then the x window
-// of a dense diagonal shape (the two are never live at the same time).
-__host__ __device__ inline int smem_rp_ints(int rows_cap) { return (rows_cap + 8 + 3) & ~3; }
-// per-row sums; at least one slot per warp for the long-row reduction
-__host__ __device__ inline int smem_racc_floats(int rows_cap) { return ((rows_cap < 32 ? 32 : rows_cap) + 3) & ~3; }
-__host__ __device__ inline int smem_buf_floats(int rows_cap, int nnz_cap, int max_span)
-{
-    int xw = rows_cap + max_span + 16;
-    int b = nnz_cap > xw ? nnz_cap : xw;
-    return (b + 3) & ~3;
-}
+constexpr int kRPT = 4;   // rows per lane group per pass
 
-inline size_t spmv_smem_bytes_impl(int rows_cap, int nnz_cap, int max_span)
-{
-    return sizeof(int) * (size_t)smem_rp_ints(rows_cap) + sizeof(float) * (size_t)smem_racc_floats(rows_cap) +
-           sizeof(float) * (size_t)smem_buf_floats(rows_cap, nnz_cap, max_span) + 16;
-}
-
-
-constexpr int kU = 8;   // loads in flight per thread per staging round
+__host__ __device__ inline int tile_rows_for(int lanes) { return (kBlock / lanes) * kRPT; }
 
 template <bool SIGNED>
 __device__ __forceinline__ float gather(const float *__restrict__ x, int c)
 {
     if (SIGNED) {
-        float v = __ldg(x + (c >> 1));
+        const float v = __ldg(x + (c >> 1));
         return (c & 1) ? v : -v;
     }
     return __ldg(x + c);
 }
+
+// Programmatic dependent launch: a kernel reads only immutable plan data
+// before wait_prior_grid(); x is read and y written after it, when every grid
+// earlier in the stream has finished and its writes are visible.
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 __device__ __forceinline__ float warp_sum(float v)
 {
@@ -50,74 +52,155 @@ __device__ __forceinline__ float warp_sum(float v)
     return v;
 }
 
-// Adds the dense-diagonal terms of rows [r0, r0+nr) of one tile to racc[] (in
-// shared memory), staging each shape's x window in xw[].  All threads call.
-__device__ __forceinline__ void tile_diagonals(const DevPlan &p, const float *__restrict__ x,
-                                               int r0, int nr, float *racc, float *xw)
+// Tile-relative row pointers / CSR words read from global memory.
+struct GlobalSrc {
+    const int *rp;     // &rowptr[row0]
+    const int *cw;     // &cols[nz0]
+    int nz0;
+    __device__ __forceinline__ int row(int r) const { return __ldg(rp + r) - nz0; }
+    __device__ __forceinline__ int word(int j) const { return __ldg(cw + j); }
+};
+
+// The same read from a shared-memory copy (aligned-down starts: rp_off / cw_off).
+struct SharedSrc {
+    const int *rp;
+    const int *cw;
+    int nz0;
+    __device__ __forceinline__ int row(int r) const { return rp[r] - nz0; }
+    __device__ __forceinline__ int word(int j) const { return cw[j]; }
+};
+
+// Adds the dense-diagonal terms of rows row0 + base + k*G + g (k < kRPT) to
+// acc[k]; the shape's offsets are split over the row's lanes.  Offset `off`
+// of a shape covers rows [xStart + max(0,-off), xStop - max(0,off)).
+template <int LANES>
+__device__ __forceinline__ void diag_terms(const DevPlan &p, const float *__restrict__ x, int row0,
+                                           int nr, int base, int g, int lane, float (&acc)[kRPT])
 {
-    const int tid = threadIdx.x;
-    const int r1 = r0 + nr;
-    if (r1 <= p.row_start || r0 >= p.row_stop) return;
+    constexpr int G = kBlock / LANES;
+    const int lo = row0 + base, hi = row0 + min(nr, base + G * kRPT);   // rows of this pass
+    if (hi <= p.row_start || lo >= p.row_stop) return;
     for (int s = 0; s < p.dia_shapes; ++s) {
-        const int4 sh = __ldg(p.shapes + s);     // xStart, xStop, yStart, Msub
-        const int ra = max(r0, sh.x), rb = min(r1, sh.y);
-        if (ra >= rb) continue;                  // uniform across the CTA
+        const int4 sh = __ldg(p.shapes + s);          // xStart, xStop, yStart, Msub
+        if (hi <= sh.x || lo >= sh.y) continue;       // uniform across the CTA
         const int2 dr = __ldg(p.shape_dias + s);
-        const int omin = __ldg(p.offsets + dr.x), omax = __ldg(p.offsets + dr.y - 1);
-        const int cbase = sh.z - sh.x;           // col = row + cbase + off
-        int lo = ra + cbase + omin, hi = rb - 1 + cbase + omax;   // inclusive
-        lo = max(lo, sh.z);
-        hi = min(hi, sh.z + sh.w - 1);
-        if (lo <= hi) {
-            // x[lo..hi] -> xw[0..]; 16-byte loads on the aligned interior.
-            const int a4 = (lo + 3) & ~3, b4 = (hi + 1) & ~3;   // [a4, b4) aligned
-            const bool x16 = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-            if (x16 && a4 < b4) {
-                const float4 *x4 = reinterpret_cast<const float4 *>(x + a4);
-                const int n4 = (b4 - a4) >> 2;
-                for (int i = tid; i < n4; i += kBlock) {
-                    float4 v = __ldg(x4 + i);
-                    float *d = xw + (a4 - lo) + 4 * i;
-                    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-                }
-                for (int i = lo + tid; i < a4; i += kBlock) xw[i - lo] = __ldg(x + i);
-                for (int i = b4 + tid; i <= hi; i += kBlock) xw[i - lo] = __ldg(x + i);
-            } else {
-                for (int i = lo + tid; i <= hi; i += kBlock) xw[i - lo] = __ldg(x + i);
+        const int cb = sh.z - sh.x;                   // column = row + cb + off
+        for (int n = dr.x + lane; n < dr.y; n += LANES) {
+            const int off = __ldg(p.offsets + n);
+            const int a = sh.x + max(0, -off), b = sh.y - max(0, off);
+            float v[kRPT];
+#pragma unroll
+            for (int k = 0; k < kRPT; ++k) {
+                const int rl = base + k * G + g, r = row0 + rl;
+                v[k] = (rl < nr && r >= a && r < b) ? __ldg(x + r + cb + off) : 0.f;
             }
+#pragma unroll
+            for (int k = 0; k < kRPT; ++k) acc[k] += v[k];
         }
-        __syncthreads();
-        if (lo <= hi) {
-            for (int r = ra + tid; r < rb; r += kBlock) {
-                float acc = racc[r - r0];
-                const int cb = r + cbase;
-                for (int n = dr.x; n < dr.y; ++n) {
-                    const int c = cb + __ldg(p.offsets + n);
-                    if (c >= lo && c <= hi) acc += xw[c - lo];
-                }
-                racc[r - r0] = acc;
-            }
-        }
-        __syncthreads();
     }
 }
 
+// One pass (kRPT rows per lane group) of a TILE_L<LANES> tile.
+template <bool SIGNED, int LANES, class Src>
+__device__ __forceinline__ void rows_pass(const DevPlan &p, int row0, int nr, int base,
+                                          const Src &src, const float *__restrict__ x,
+                                          float *__restrict__ y, bool wait)
+{
+    constexpr int G = kBlock / LANES;
+    const int g = threadIdx.x / LANES;
+    const int lane = threadIdx.x & (LANES - 1);
+    int rb[kRPT], re[kRPT];
+#pragma unroll
+    for (int k = 0; k < kRPT; ++k) {
+        const int r = base + k * G + g;
+        const bool ok = r < nr;
+        rb[k] = ok ? src.row(r) : 0;
+        re[k] = ok ? src.row(r + 1) : 0;
+    }
+    // first round of CSR words: immutable plan data, loaded before the wait
+    int c[kRPT];
+#pragma unroll
+    for (int k = 0; k < kRPT; ++k) {
+        const int j = rb[k] + lane;
+        c[k] = j < re[k] ? src.word(j) : -1;
+    }
+    if (wait) wait_prior_grid();
+    float acc[kRPT];
+#pragma unroll
+    for (int k = 0; k < kRPT; ++k) acc[k] = 0.f;
+    if (p.dia_shapes > 0) diag_terms<LANES>(p, x, row0, nr, base, g, lane, acc);
+    for (int j0 = lane;;) {
+        float v[kRPT];
+#pragma unroll
+        for (int k = 0; k < kRPT; ++k) v[k] = c[k] >= 0 ? gather<SIGNED>(x, c[k]) : 0.f;
+#pragma unroll
+        for (int k = 0; k < kRPT; ++k)
+            if (c[k] >= 0) acc[k] += v[k];
+        j0 += LANES;
+        bool more = false;
+#pragma unroll
+        for (int k = 0; k < kRPT; ++k) {
+            const int j = rb[k] + j0;
+            const bool ok = j < re[k];
+            c[k] = ok ? src.word(j) : -1;
+            more |= ok;
+        }
+        if (!__any_sync(0xffffffffu, more)) break;
+    }
+#pragma unroll
+    for (int k = 0; k < kRPT; ++k) {
+#pragma unroll
+        for (int o = LANES / 2; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+        const int r = base + k * G + g;
+        if (lane == 0 && r < nr) y[row0 + r] = acc[k];
+    }
+}
+
+template <bool SIGNED, int LANES, class Src>
+__device__ __forceinline__ void tile_rows(const DevPlan &p, const Tile &t, const Src &src,
+                                          const float *__restrict__ x, float *__restrict__ y,
+                                          bool wait)
+{
+    constexpr int G = kBlock / LANES;
+    const int nr = tile_nrows(t);
+    for (int base = 0; base < nr; base += G * kRPT)
+        rows_pass<SIGNED, LANES>(p, t.row0, nr, base, src, x, y, wait);
+}
+
+// One row with more entries than the planner's per-tile limit: the whole CTA
+// strides over it; warp sums are combined in warp order.
 template <bool SIGNED>
 __device__ void long_row(const DevPlan &p, const Tile &t, const float *__restrict__ x,
-                         float *__restrict__ y, float *red)
+                         float *__restrict__ y, bool wait)
 {
+    __shared__ float red[kBlock / 32];
+    constexpr int U = 8;
     const int tid = threadIdx.x;
     const int *__restrict__ cols = p.cols + t.nz0;
     float acc = 0.f;
-    for (int base = 0; base < t.nnz; base += kBlock * kU) {
-        int c[kU];
+    bool waited = !wait;
+    // dense-diagonal terms of the row first (thread-strided offsets)
+    if (!waited) { wait_prior_grid(); waited = true; }
+    const int r = t.row0;
+    if (p.dia_shapes > 0 && r >= p.row_start && r < p.row_stop)
+        for (int s = 0; s < p.dia_shapes; ++s) {
+            const int4 sh = __ldg(p.shapes + s);
+            if (r < sh.x || r >= sh.y) continue;
+            const int2 dr = __ldg(p.shape_dias + s);
+            for (int n = dr.x + tid; n < dr.y; n += kBlock) {
+                const int c = r - sh.x + sh.z + __ldg(p.offsets + n);
+                if (c >= sh.z && c < sh.z + sh.w) acc += __ldg(x + c);
+            }
+        }
+    for (int base = 0; base < t.nnz; base += kBlock * U) {
+        int c[U];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            int i = base + u * kBlock + tid;
+        for (int u = 0; u < U; ++u) {
+            const int i = base + u * kBlock + tid;
             c[u] = i < t.nnz ? __ldg(cols + i) : -1;
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u)
+        for (int u = 0; u < U; ++u)
             if (c[u] >= 0) acc += gather<SIGNED>(x, c[u]);
     }
     acc = warp_sum(acc);
@@ -126,101 +209,34 @@ __device__ void long_row(const DevPlan &p, const Tile &t, const float *__restric
     if (tid < 32) {
         float v = tid < kBlock / 32 ? red[tid] : 0.f;
         v = warp_sum(v);
-        if (tid == 0) {
-            const int r = t.row0;
-            if (p.dia_shapes > 0 && r >= p.row_start && r < p.row_stop) {
-                for (int s = 0; s < p.dia_shapes; ++s) {
-                    const int4 sh = __ldg(p.shapes + s);
-                    if (r < sh.x || r >= sh.y) continue;
-                    const int2 dr = __ldg(p.shape_dias + s);
-                    for (int n = dr.x; n < dr.y; ++n) {
-                        int col = r - sh.x + sh.z + __ldg(p.offsets + n);
-                        if (col >= sh.z && col < sh.z + sh.w) v += __ldg(x + col);
-                    }
-                }
-            }
-            y[r] = v;
-        }
+        if (tid == 0) y[r] = v;
+    }
+    __syncthreads();
+}
+
+template <bool SIGNED, class Src>
+__device__ __forceinline__ void run_tile_src(const DevPlan &p, const Tile &t, const Src &src,
+                                             const float *__restrict__ x, float *__restrict__ y,
+                                             bool wait)
+{
+    switch (tile_kind(t)) {
+    case TILE_L1: tile_rows<SIGNED, 1>(p, t, src, x, y, wait); break;
+    case TILE_L2: tile_rows<SIGNED, 2>(p, t, src, x, y, wait); break;
+    case TILE_L4: tile_rows<SIGNED, 4>(p, t, src, x, y, wait); break;
+    case TILE_L8: tile_rows<SIGNED, 8>(p, t, src, x, y, wait); break;
+    case TILE_L16: tile_rows<SIGNED, 16>(p, t, src, x, y, wait); break;
+    case TILE_L32: tile_rows<SIGNED, 32>(p, t, src, x, y, wait); break;
+    default: long_row<SIGNED>(p, t, x, y, wait); break;
     }
 }
 
-// Processes one tile (any kind).  Shared by the single-plan and the batched
-// kernels so a matrix gives bit-identical y alone and inside a batch.
+// A tile read straight from global memory.
 template <bool SIGNED>
-__device__ void run_tile(const DevPlan &p, const Tile &t, const float *__restrict__ x,
-                         float *__restrict__ y, char *smem)
+__device__ __forceinline__ void run_tile(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                                         float *__restrict__ y, bool wait = true)
 {
-    const int tid = threadIdx.x;
-    int *rp = reinterpret_cast<int *>(smem);
-    float *racc = reinterpret_cast<float *>(rp + smem_rp_ints(p.rows_cap));
-    float *vals = racc + smem_racc_floats(p.rows_cap);
-    float *xw = vals;   // reused once the CSR terms are summed
-    const int kind = tile_kind(t);
-    if (kind == TILE_LONG) {
-        long_row<SIGNED>(p, t, x, y, racc);
-        return;
-    }
-    const int nr = tile_nrows(t), nz = t.nnz, r0 = t.row0, nz0 = t.nz0;
-
-    // Phase A: row pointers and CSR entries of the tile, loads batched so
-    // that each thread keeps kU requests in flight.
-    {
-        int v[kU];
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            int i = u * kBlock + tid;
-            v[u] = i <= nr ? __ldg(p.rowptr + r0 + i) : 0;
-        }
-        for (int base = 0; base < nz; base += kBlock * kU) {
-            int c[kU];
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                int i = base + u * kBlock + tid;
-                c[u] = i < nz ? __ldg(p.cols + nz0 + i) : 0;
-            }
-            float g[kU];
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                int i = base + u * kBlock + tid;
-                g[u] = i < nz ? gather<SIGNED>(x, c[u]) : 0.f;
-            }
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                int i = base + u * kBlock + tid;
-                if (i < nz) vals[i] = g[u];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            int i = u * kBlock + tid;
-            if (i <= nr) rp[i] = v[u] - nz0;
-        }
-    }
-    __syncthreads();
-
-    // Phase B: per-row sums of the staged entries.
-    if (kind == TILE_SCALAR) {
-        for (int r = tid; r < nr; r += kBlock) {
-            float s = 0.f;
-            const int e = rp[r + 1];
-            for (int j = rp[r]; j < e; ++j) s += vals[j];
-            racc[r] = s;
-        }
-    } else {
-        const int lane = tid & 31, warp = tid >> 5;
-        for (int r = warp; r < nr; r += kBlock / 32) {
-            float s = 0.f;
-            const int e = rp[r + 1];
-            for (int j = rp[r] + lane; j < e; j += 32) s += vals[j];
-            s = warp_sum(s);
-            if (lane == 0) racc[r] = s;
-        }
-    }
-    __syncthreads();
-
-    // Phase C: dense diagonals, then one coalesced store of y.
-    if (p.dia_shapes > 0) tile_diagonals(p, x, r0, nr, racc, xw);
-    for (int r = tid; r < nr; r += kBlock) y[r0 + r] = racc[r];
+    const GlobalSrc src{p.rowptr + t.row0, p.cols + t.nz0, t.nz0};
+    run_tile_src<SIGNED>(p, t, src, x, y, wait);
 }
 
 }  // namespace tc

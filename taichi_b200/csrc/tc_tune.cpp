@@ -1,0 +1,192 @@
+// tc_tune.cpp -- per-matrix autotuner for the partition threshold and the
+// multiply's tile shape.
+//
+// The reference hard-codes the dense-diagonal threshold (0.6, TaiChi.cu:757)
+// and derives one vector width per matrix (TaiChi.cu:1390-1394).  The tuner
+// measures instead: it partitions the matrix on the GPU at several density
+// thresholds, then, on the best format, tries tile shapes (rows per tile,
+// most lanes per row, resident CTAs per SM), timing each candidate with CUDA
+// events over back-to-back multiplies.  Every candidate computes the same
+// product (the format only moves entries between the diagonal and CSR parts),
+// so the choice is purely a speed decision.  Results are cached per matrix
+// fingerprint for the life of the process.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "tc_internal.h"
+
+namespace {
+
+std::mutex g_mu;
+std::unordered_map<uint64_t, tc_tune_result> g_cache;
+
+uint64_t mix(uint64_t h, uint64_t v)
+{
+    h ^= v + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+    return h;
+}
+
+// Sizes plus a strided sample of the row pointers and column indices.
+uint64_t fingerprint(int M, int N, int64_t nnz, const int *rp, const int *col)
+{
+    uint64_t h = mix(mix(mix(0x5eed, (uint64_t)M), (uint64_t)N), (uint64_t)nnz);
+    const int64_t sr = std::max<int64_t>(1, M / 1024), sc = std::max<int64_t>(1, nnz / 4096);
+    for (int64_t r = 0; r <= M; r += sr) h = mix(h, (uint64_t)(uint32_t)rp[r]);
+    for (int64_t j = 0; j < nnz; j += sc) h = mix(h, (uint64_t)(uint32_t)col[j]);
+    return h;
+}
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer() { cudaEventCreate(&a); cudaEventCreate(&b); }
+    ~Timer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+};
+
+// Mean device time of one multiply (us) over `reps` launches after warm-up.
+tc_status time_plan(const tc_plan *p, const float *dx, float *dy, cudaStream_t s, int reps, double *us)
+{
+    Timer t;
+    for (int i = 0; i < 3; ++i) TC_CHECK(tc_spmv(p, dx, dy, s));
+    TC_CUDA(cudaEventRecord(t.a, s));
+    for (int i = 0; i < reps; ++i) TC_CHECK(tc_spmv(p, dx, dy, s));
+    TC_CUDA(cudaEventRecord(t.b, s));
+    TC_CUDA(cudaEventSynchronize(t.b));
+    float ms = 0.f;
+    TC_CUDA(cudaEventElapsedTime(&ms, t.a, t.b));
+    *us = 1e3 * ms / reps;
+    return TC_OK;
+}
+
+}  // namespace
+
+using tc::fail;
+
+extern "C" tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const int *col,
+                             const tc_params *base, int max_trials, void *stream,
+                             tc_tune_result *out)
+{
+    if (!rowptr || (nnz && !col) || !out || M <= 0 || N <= 0)
+        return fail(TC_ERR_INVALID, "tc_tune: bad arguments");
+    tc_params b0;
+    tc_params_default(&b0);
+    if (base) b0 = *base;
+    const uint64_t fp = fingerprint(M, N, nnz, rowptr, col);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_cache.find(fp);
+        if (it != g_cache.end()) {
+            *out = it->second;
+            out->trials = 0;
+            out->cached = 1;
+            return TC_OK;
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    float *dx = nullptr, *dy = nullptr;
+    if (cudaMalloc(&dx, sizeof(float) * ((size_t)N + 4)) != cudaSuccess ||
+        cudaMalloc(&dy, sizeof(float) * ((size_t)M + 4)) != cudaSuccess) {
+        if (dx) cudaFree(dx);
+        return fail(TC_ERR_ALLOC, "tuner vectors");
+    }
+    TC_CUDA(cudaMemsetAsync(dx, 0, sizeof(float) * (size_t)N, s));
+    const int reps = 20;
+    int trials = 0;
+    if (max_trials <= 0) max_trials = 32;
+    tc_tune_result best{};
+    best.params = b0;
+    best.spmv_us = 1e30;
+    tc_status st = TC_OK;
+
+    // 1. density threshold (partition) with the base tile shape
+    const double dens[] = {b0.density, 0.5, 0.7, 0.8, 0.9, 0.95};
+    tc_plan *best_plan = nullptr;
+    for (int k = 0; k < (int)(sizeof dens / sizeof dens[0]); ++k) {
+        const double d = dens[k];
+        if (trials >= max_trials) break;
+        if (k > 0 && std::fabs(d - b0.density) < 1e-12) continue;     // already timed
+        tc_params q = b0;
+        q.density = d;
+        q.flags |= TC_FLAG_KEEP_HOST;
+        tc_plan *p = nullptr;
+        st = tc_plan_create(M, N, nnz, rowptr, col, nullptr, 0, &q, stream, &p);
+        if (st != TC_OK) break;
+        double us = 0;
+        st = time_plan(p, dx, dy, s, reps, &us);
+        ++trials;
+        if (k == 0) best.default_us = us;
+        const bool no_shapes = p->corners.empty();
+        if (st == TC_OK && us < best.spmv_us) {
+            best.spmv_us = us;
+            best.params = q;
+            if (best_plan) tc_plan_destroy(best_plan);
+            best_plan = p;
+        } else {
+            tc_plan_destroy(p);
+        }
+        if (st != TC_OK) break;
+        if (no_shapes) break;            // no thumbnail shape: the threshold changes nothing
+    }
+    // 2. tile shape on the best format
+    if (st == TC_OK && best_plan) {
+        tc_format f{};
+        std::vector<int> rp((size_t)M + 1), cw((size_t)std::max<int64_t>(best_plan->nnz_csr, 1));
+        st = tc_plan_export(best_plan, nullptr, nullptr, nullptr, nullptr, nullptr, rp.data(), cw.data());
+        f.dia_shapes = best_plan->dia_shapes; f.num_negs = best_plan->num_negs;
+        f.dense_nnz = best_plan->dense_nnz; f.zero_elements = best_plan->zero_elements;
+        f.sparse_nnz = best_plan->sparse_nnz; f.row_start = best_plan->row_start;
+        f.row_stop = best_plan->row_stop;
+        f.xStart = best_plan->h_xStart.data(); f.yStart = best_plan->h_yStart.data();
+        f.xStop = best_plan->h_xStop.data(); f.nDiasPtr = best_plan->h_nDiasPtr.data();
+        f.neg_offsets = best_plan->h_offsets.data();
+        f.csrRow = rp.data(); f.csrCol = cw.data();
+        const int rows_c[] = {256, 512, 1024, 2048};
+        const int lanes_c[] = {32, 8};
+        const int cps_c[] = {4, 2, 8};
+        for (int cps : cps_c)
+            for (int lanes : lanes_c)
+                for (int rows : rows_c) {
+                    if (st != TC_OK || trials >= max_trials) break;
+                    tc_params q = best.params;
+                    q.tile_rows = rows; q.max_lanes = lanes; q.ctas_per_sm = cps;
+                    q.flags &= ~TC_FLAG_KEEP_HOST;
+                    if (q.tile_rows == best.params.tile_rows && q.max_lanes == best.params.max_lanes &&
+                        q.ctas_per_sm == best.params.ctas_per_sm)
+                        continue;
+                    tc_plan *p = nullptr;
+                    st = tc_plan_from_format(M, N, &f, &q, stream, &p);
+                    if (st != TC_OK) break;
+                    double us = 0;
+                    st = time_plan(p, dx, dy, s, reps, &us);
+                    ++trials;
+                    if (st == TC_OK && us < best.spmv_us) { best.spmv_us = us; best.params = q; }
+                    tc_plan_destroy(p);
+                }
+    }
+    if (best_plan) tc_plan_destroy(best_plan);
+    cudaFree(dx);
+    cudaFree(dy);
+    if (st != TC_OK) return st;
+    best.params.flags &= ~TC_FLAG_KEEP_HOST;
+    best.trials = trials;
+    best.cached = 0;
+    best.fingerprint = fp;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_cache[fp] = best;
+    }
+    *out = best;
+    return TC_OK;
+}
+
+extern "C" void tc_tune_cache_clear(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_cache.clear();
+}

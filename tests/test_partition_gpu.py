@@ -199,3 +199,11 @@ def test_compat_partition_dia_shape(tc, dev, golden):
     want, wval = oracle.partition(M, N, rp, col)
     np.testing.assert_array_equal(val == FLT_MAX, wval == FLT_MAX)
     assert sum(t.numZeroNeg[i] for i in range(t.neg)) == rec["zero_elements"]
+
+
+def test_invalid_input_rejected(tc, dev):
+    rp = np.array([0, 1, 2], np.int32)
+    with pytest.raises(tc.TcError):
+        tc.Plan.from_csr(2, 5, rp, np.array([0, 7], np.int32))        # column >= N
+    with pytest.raises(tc.TcError):
+        tc.Plan.from_csr(2, 5, np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32))

@@ -25,6 +25,7 @@ def run_spmv(plan, x, M, dev):
     y = torch.full((M,), float("nan"), dtype=torch.float32, device=dev)
     plan.spmv(xd, y)
     torch.cuda.synchronize()
+    plan.check()
     return y.cpu().numpy()
 
 
