@@ -167,6 +167,58 @@ __device__ __forceinline__ void tile_rows(const DevPlan &p, const Tile &t, const
         rows_pass<SIGNED, LANES>(p, t.row0, nr, base, src, x, y, wait);
 }
 
+// One lane per row: a thread owns up to kRPT consecutive rows and walks
+// their CSR words straight through (no lock-step rounds), after adding each
+// row's dense-diagonal terms.  Same per-row order as rows_pass.
+template <bool SIGNED, class Src>
+__device__ __forceinline__ void tile_rows1(const DevPlan &p, const Tile &t, const Src &src,
+                                           const float *__restrict__ x, float *__restrict__ y,
+                                           bool wait)
+{
+    const int nr = tile_nrows(t), row0 = t.row0;
+    for (int base = 0; base < nr; base += kBlock * kRPT) {
+        const int n = min(nr - base, kBlock * kRPT);
+        const int q = (n + kBlock - 1) / kBlock;            // rows per thread, 1..kRPT
+        const int lo = base + (int)threadIdx.x * q;
+        const int hi = min(lo + q, base + n);               // this thread's rows [lo, hi)
+        int e[kRPT + 1];
+#pragma unroll
+        for (int k = 0; k <= kRPT; ++k) e[k] = lo < hi ? src.row(min(lo + k, hi)) : 0;
+        if (wait) wait_prior_grid();
+        float acc[kRPT];
+#pragma unroll
+        for (int k = 0; k < kRPT; ++k) acc[k] = 0.f;
+        if (p.dia_shapes > 0 && lo < hi && row0 + hi > p.row_start && row0 + lo < p.row_stop) {
+            for (int s = 0; s < p.dia_shapes; ++s) {
+                const int4 sh = __ldg(p.shapes + s);        // xStart, xStop, yStart, Msub
+                if (row0 + hi <= sh.x || row0 + lo >= sh.y) continue;
+                const int2 dr = __ldg(p.shape_dias + s);
+                const int cb = sh.z - sh.x;
+                for (int d = dr.x; d < dr.y; ++d) {
+                    const int off = __ldg(p.offsets + d);
+                    const int a = sh.x + max(0, -off), b = sh.y - max(0, off);
+                    float v[kRPT];
+#pragma unroll
+                    for (int k = 0; k < kRPT; ++k) {
+                        const int r = row0 + lo + k;
+                        v[k] = (lo + k < hi && r >= a && r < b) ? __ldg(x + r + cb + off) : 0.f;
+                    }
+#pragma unroll
+                    for (int k = 0; k < kRPT; ++k) acc[k] += v[k];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kRPT; ++k) {
+#pragma unroll 4
+            for (int j = e[k]; j < e[k + 1]; ++j) acc[k] += gather<SIGNED>(x, src.word(j));
+        }
+#pragma unroll
+        for (int k = 0; k < kRPT; ++k)
+            if (lo + k < hi) y[row0 + lo + k] = acc[k];
+    }
+}
+
 // One row with more entries than the planner's per-tile limit: the whole CTA
 // strides over it; warp sums are combined in warp order.
 template <bool SIGNED>
@@ -220,7 +272,7 @@ __device__ __forceinline__ void run_tile_src(const DevPlan &p, const Tile &t, co
                                              bool wait)
 {
     switch (tile_kind(t)) {
-    case TILE_L1: tile_rows<SIGNED, 1>(p, t, src, x, y, wait); break;
+    case TILE_L1: tile_rows1<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_L2: tile_rows<SIGNED, 2>(p, t, src, x, y, wait); break;
     case TILE_L4: tile_rows<SIGNED, 4>(p, t, src, x, y, wait); break;
     case TILE_L8: tile_rows<SIGNED, 8>(p, t, src, x, y, wait); break;
