@@ -312,6 +312,177 @@ def run_ours(args, rank, world, local_rank):
         p.close()
 
 
+def _events(torch, stream):
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    return a, b
+
+
+def run_spmm(args):
+    """Batched right-hand sides: Y = A X, X 4,194,304 x 64 FP32 (R-MAT scale 22)."""
+    import torch
+    import taichi_b200 as tc
+    dev = torch.device("cuda", 0)
+    M, rp, col = tc.gen_rmat(22, 16, 0.499, 0.001, 0.001, seed=1)
+    N, k = M, 64
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    info = plan.info()
+    X = torch.empty((N, k), device=dev).uniform_(-1, 1)
+    Y = torch.empty((M, k), device=dev)
+    stream = torch.cuda.Stream(dev)
+    for _ in range(max(args.warmup, 3)):
+        plan.spmm(X, Y, stream=stream)
+    torch.cuda.synchronize()
+    a, b = _events(torch, stream)
+    steps = min(args.steps, 200)
+    a.record(stream)
+    for _ in range(steps):
+        plan.spmm(X, Y, stream=stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    nbytes = 4 * (M + 1) + 4 * info["nnz_csr"] + 4 * k * N + 4 * k * M
+    peak, kind = load_peaks()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    print(json.dumps({"form": "spmm", "metric": "SpMM GB/s (k=64) at R-MAT scale 22",
+                      "value": round(gbs, 1), "unit": "GB/s", "ms_per_step": ms, "steps": steps,
+                      "frac_of_hbm": round(gbs / peak, 4), "peak": peak, "peak_kind": kind,
+                      "config": {"M": M, "nnz": int(rp[M]), "k": k, "bytes": nbytes,
+                                 "dia_shapes": info["dia_shapes"]}}), flush=True)
+
+
+def pool_matrices(kind, count, seed):
+    """Seeded matrix pools of the batched (kind='batch') and served
+    (kind='serve') workloads."""
+    import taichi_b200 as tc
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        if kind == "batch":
+            n = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+            if i % 2 == 0:
+                sc = max(10, int(round(np.log2(n))))
+                M, rp, col = tc.gen_rmat(sc, 8, 0.499, 0.001, 0.001, seed=seed * 1000 + i)
+                out.append(("rmat%d" % sc, M, rp, col))
+            else:
+                kk = int(rng.integers(1, 17))
+                rp, col = tc.gen_banded(n, kk, 4, seed=seed * 1000 + i)
+                out.append(("band%d_k%d" % (n, kk), n, rp, col))
+        else:
+            if i < count // 2:
+                sc = 14 + (i * 9) // (count // 2)          # scales 14..22
+                M, rp, col = tc.gen_rmat(sc, 16, 0.499, 0.001, 0.001, seed=seed * 1000 + i)
+                out.append(("rmat%d" % sc, M, rp, col))
+            else:
+                n = int(np.exp(rng.uniform(np.log(1e4), np.log(4e6))))
+                kk = int(rng.integers(1, 17))
+                rr = int(rng.integers(2, 13))
+                rp, col = tc.gen_banded(n, kk, rr, seed=seed * 1000 + i)
+                out.append(("band%d_k%d_r%d" % (n, kk, rr), n, rp, col))
+    return out
+
+
+def run_batched(args):
+    """256 matrices of uneven size in one persistent, graph-captured launch,
+    autotuned per matrix, against one launch per matrix."""
+    import ctypes as C
+    import torch
+    import taichi_b200 as tc
+    dev = torch.device("cuda", 0)
+    mats = pool_matrices("batch", 256, 7)
+    t0 = time.perf_counter()
+    plans, xs, ys, nbytes, tuned = [], [], [], 0, 0
+    for name, M, rp, col in mats:
+        r = tc.tune(M, M, rp, col, max_trials=args.tune_trials) if args.tune_trials > 0 else None
+        prm = r.params if r is not None else tc.params()
+        tuned += r is not None
+        p = tc.Plan.from_csr(M, M, rp, col, prm=prm)
+        plans.append(p)
+        xs.append(torch.empty(M, device=dev).uniform_(-1, 1))
+        ys.append(torch.empty(M, device=dev))
+        nbytes += p.info()["spmv_bytes"]
+    build_s = time.perf_counter() - t0
+    n = len(plans)
+    H = (C.c_void_p * n)(*[p.handle.value for p in plans])
+    X = (C.c_void_p * n)(*[x.data_ptr() for x in xs])
+    Yp = (C.c_void_p * n)(*[y.data_ptr() for y in ys])
+    b = C.c_void_p()
+    tc.check(tc.lib().tc_batch_create(n, H, X, Yp, C.byref(b)))
+    stream = torch.cuda.Stream(dev)
+    for _ in range(3):
+        tc.check(tc.lib().tc_batch_graph_launch(b, C.c_void_p(stream.cuda_stream)))
+    torch.cuda.synchronize()
+    steps = min(args.steps, 500)
+    a, e = _events(torch, stream)
+    a.record(stream)
+    for _ in range(steps):
+        tc.check(tc.lib().tc_batch_graph_launch(b, C.c_void_p(stream.cuda_stream)))
+    e.record(stream)
+    torch.cuda.synchronize()
+    ms_batch = a.elapsed_time(e) / steps
+    # plain: one multiply launch per matrix, back to back (captured in a graph)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        for p, x, y in zip(plans, xs, ys):
+            p.spmv(x, y, stream=torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        g.replay()
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(steps):
+            g.replay()
+        e.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = a.elapsed_time(e) / steps
+    tc.check(tc.lib().tc_batch_destroy(b))
+    print(json.dumps({"form": "batched", "matrices": n, "rows": int(sum(m[1] for m in mats)),
+                      "nnz": int(sum(int(m[2][-1]) for m in mats)),
+                      "batch_ms": ms_batch, "plain_ms": ms_plain,
+                      "batch_spmv_per_s": round(n / (ms_batch * 1e-3)),
+                      "plain_spmv_per_s": round(n / (ms_plain * 1e-3)),
+                      "batch_gbs": round(nbytes / (ms_batch * 1e-3) / 1e9, 1),
+                      "plain_gbs": round(nbytes / (ms_plain * 1e-3) / 1e9, 1),
+                      "speedup": round(ms_plain / ms_batch, 2), "tuned": tuned,
+                      "build_s": round(build_s, 1)}), flush=True)
+
+
+def run_served(args):
+    """20,000 requests, Poisson arrivals, Zipf(1.1) over a 48-matrix resident
+    pool; continuous batching against one synchronous request at a time."""
+    import torch
+    import taichi_b200 as tc
+    mats = pool_matrices("serve", 48, 11)
+    srv = tc.Server(contexts=3, max_batch=64, arena_bytes=512 << 20, hbm_budget=96 << 30)
+    plans, ids = [], []
+    for name, M, rp, col in mats:
+        p = tc.Plan.from_csr(M, M, rp, col)
+        plans.append(p)
+        ids.append(srv.admit(p))
+    rng = np.random.default_rng(5)
+    # two pinned x and y buffers per matrix, reused round-robin
+    xb = [[torch.empty(m[1]).uniform_(-1, 1).pin_memory() for _ in range(2)] for m in mats]
+    yb = [[torch.empty(m[1]).pin_memory() for _ in range(2)] for m in mats]
+    ranks = np.arange(1, len(mats) + 1, dtype=np.float64)
+    pz = ranks ** -1.1
+    pz /= pz.sum()
+    nreq = args.requests
+    results = []
+    for rate in args.rates:
+        matrix = rng.choice(len(mats), size=nreq, p=pz)
+        arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
+        xs = [xb[m][i & 1] for i, m in enumerate(matrix)]
+        ys = [yb[m][i & 1] for i, m in enumerate(matrix)]
+        row = {"rate": rate}
+        for mode, name in ((0, "batched"), (1, "plain")):
+            st, lat = srv.run(arrival, [ids[m] for m in matrix], xs, ys, mode=mode)
+            row[name] = {k: round(st[k], 4) for k in ("spmv_per_s", "p50_ms", "p99_ms", "mean_batch")}
+        results.append(row)
+        print(json.dumps(row), flush=True)
+    print(json.dumps({"form": "served", "requests": nreq, "pool": len(mats),
+                      "pool_rows": int(sum(m[1] for m in mats)), "results": results}), flush=True)
+    srv.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,9 +490,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat20")
+    ap.add_argument("--form", default="plain", choices=["plain", "spmm", "batched", "served"])
+    ap.add_argument("--tune-trials", type=int, default=8)
+    ap.add_argument("--requests", type=int, default=20000)
+    ap.add_argument("--rates", type=float, nargs="+", default=[2000, 5000, 10000, 20000])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    if args.impl == "ours" and args.form != "plain":
+        {"spmm": run_spmm, "batched": run_batched, "served": run_served}[args.form](args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

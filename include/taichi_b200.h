@@ -54,6 +54,9 @@ typedef struct tc_params {
     int tile_nnz;         /* rows with more CSR entries get a CTA each (2048)  */
     int max_lanes;        /* most lanes the planner gives one row: 1..32 (32)  */
     int ctas_per_sm;      /* resident CTAs per SM of the multiply grid (4)     */
+    int tile_mode;        /* 0: rows and entries split evenly over a CTA's
+                             threads (merge path); 1: lanes per row chosen
+                             from the tile's row lengths (1)                   */
     int flags;            /* TC_FLAG_*                                         */
 } tc_params;
 
@@ -174,6 +177,16 @@ TC_API tc_status tc_trace_contours(const unsigned char *img, int H, int W, int *
 TC_API tc_status tc_read_mtx(const char *path, int *M, int *N, int64_t *nnz, int **rowptr,
                       int **col, float **val, int *ref_code);
 TC_API void tc_free(void *p);
+
+/* Synthetic benchmark matrices (no counterpart in the reference, whose
+ * datasets are external files): R-MAT graphs (each of ef * 2^scale edges
+ * picks a quadrant per level with probabilities a, b, c, 1-a-b-c) and
+ * banded patterns (dense diagonals -k..+k plus per_row random columns).
+ * Sorted, duplicate-free malloc'd CSR (free with tc_free); multi-threaded,
+ * the result depends only on the arguments. */
+TC_API tc_status tc_gen_rmat(int scale, int edge_factor, double a, double b, double c,
+                             uint64_t seed, int self_loops, int *M, int **rowptr, int **col);
+TC_API tc_status tc_gen_banded(int n, int k, int per_row, uint64_t seed, int **rowptr, int **col);
 
 /* ----------------------------------------------------------------------- */
 /* Autotuner: density threshold and tile shape, timed per matrix.           */

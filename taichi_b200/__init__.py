@@ -33,7 +33,7 @@ class Params(C.Structure):
     _fields_ = [("thumb_height", C.c_int), ("open_len", C.c_int), ("eye_size", C.c_int),
                 ("min_contour", C.c_int), ("min_shape_side", C.c_int), ("density", C.c_double),
                 ("tile_rows", C.c_int), ("tile_nnz", C.c_int), ("max_lanes", C.c_int),
-                ("ctas_per_sm", C.c_int), ("flags", C.c_int)]
+                ("ctas_per_sm", C.c_int), ("tile_mode", C.c_int), ("flags", C.c_int)]
 
 
 class Format(C.Structure):
@@ -100,6 +100,10 @@ def lib():
         L.tc_read_mtx.argtypes = [C.c_char_p, _IP, _IP, C.POINTER(C.c_int64), C.POINTER(_IP),
                                   C.POINTER(_IP), C.POINTER(C.POINTER(C.c_float)), _IP]
         L.tc_free.argtypes = [vp]
+        L.tc_gen_rmat.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_uint64, C.c_int, _IP, C.POINTER(_IP), C.POINTER(_IP)]
+        L.tc_gen_banded.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_IP),
+                                    C.POINTER(_IP)]
         L.tc_batch_create.argtypes = [C.c_int, vp, vp, vp, C.POINTER(vp)]
         L.tc_batch_run.argtypes = [vp, vp]
         L.tc_batch_graph_launch.argtypes = [vp, vp]
@@ -231,6 +235,31 @@ def tune(M, N, rowptr, col, prm=None, max_trials=32, stream=None):
                         C.byref(prm) if prm is not None else None, max_trials, _stream(stream),
                         C.byref(r)))
     return r
+
+
+def _take_csr(M, rp, ci):
+    L = lib()
+    nnz = rp[M]
+    out = (np.ctypeslib.as_array(rp, shape=(M + 1,)).copy(),
+           np.ctypeslib.as_array(ci, shape=(max(nnz, 1),))[:nnz].copy())
+    L.tc_free(C.cast(rp, C.c_void_p))
+    L.tc_free(C.cast(ci, C.c_void_p))
+    return out
+
+
+def gen_rmat(scale, edge_factor=16, a=0.499, b=0.001, c=0.001, seed=1, self_loops=False):
+    """R-MAT pattern from the library's multi-threaded generator: (M, rowptr, col)."""
+    M, rp, ci = C.c_int(), _IP(), _IP()
+    check(lib().tc_gen_rmat(scale, edge_factor, a, b, c, seed, int(self_loops), C.byref(M),
+                            C.byref(rp), C.byref(ci)))
+    return (M.value,) + _take_csr(M.value, rp, ci)
+
+
+def gen_banded(n, k, per_row, seed):
+    """Banded-plus-random pattern: (rowptr, col)."""
+    rp, ci = _IP(), _IP()
+    check(lib().tc_gen_banded(n, k, per_row, seed, C.byref(rp), C.byref(ci)))
+    return _take_csr(n, rp, ci)
 
 
 def read_mtx(path):

@@ -67,6 +67,7 @@ void tc_params_default(tc_params *p)
     p->tile_nnz = 2048;
     p->max_lanes = 32;
     p->ctas_per_sm = 4;
+    p->tile_mode = 1;
     p->flags = 0;
 }
 
@@ -79,6 +80,8 @@ static tc_status check_params(const tc_params &p)
     if (p.tile_rows < 1 || p.tile_rows > tc::kMaxTileRows)
         return fail(TC_ERR_INVALID, "tile_rows %d outside [1, %d]", p.tile_rows, tc::kMaxTileRows);
     if (p.tile_nnz < 1) return fail(TC_ERR_INVALID, "tile_nnz %d < 1", p.tile_nnz);
+    if (p.tile_mode < 0 || p.tile_mode > 1)
+        return fail(TC_ERR_INVALID, "tile_mode %d is not 0 or 1", p.tile_mode);
     if (p.ctas_per_sm < 1 || p.ctas_per_sm > 32)
         return fail(TC_ERR_INVALID, "ctas_per_sm %d outside [1, 32]", p.ctas_per_sm);
     if (p.max_lanes < 1 || p.max_lanes > 32 || (p.max_lanes & (p.max_lanes - 1)))
@@ -348,3 +351,25 @@ tc_status tc_plan_create(int M, int N, int64_t nnz, const int *rowptr, const int
 }
 
 }  // extern "C"
+
+#include <map>
+#include <mutex>
+
+namespace tc {
+
+tc_status ensure_smem(const void *kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return TC_OK;
+    int dev = 0;
+    TC_CUDA(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> done;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &v = done[{kernel, dev}];
+    if (v >= bytes) return TC_OK;
+    TC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    v = bytes;
+    return TC_OK;
+}
+
+}  // namespace tc

@@ -16,13 +16,21 @@ namespace tc {
 void set_error(const char *fmt, ...);
 tc_status fail(tc_status s, const char *fmt, ...);
 
+// On failure the runtime's last-error state is cleared too, so a failed call
+// is reported once, by the entry point that made it.
 #define TC_CUDA(call)                                                              \
     do {                                                                           \
         cudaError_t e_ = (call);                                                   \
-        if (e_ != cudaSuccess)                                                     \
+        if (e_ != cudaSuccess) {                                                   \
+            (void)cudaGetLastError();                                              \
             return ::tc::fail(TC_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__,     \
                               #call, cudaGetErrorString(e_));                      \
+        }                                                                          \
     } while (0)
+
+// Raises the dynamic shared-memory limit of `kernel` on the current device to
+// at least `bytes` (never lowers it, so earlier launches stay valid).
+tc_status ensure_smem(const void *kernel, size_t bytes);
 
 #define TC_CHECK(st)                                                               \
     do {                                                                           \
@@ -32,11 +40,13 @@ tc_status fail(tc_status s, const char *fmt, ...);
 
 // ------------------------------------------------------------- tile plan
 // A multiply tile is a run of consecutive rows processed by one CTA.  Kinds
-// TILE_L1..TILE_L32 give 1..32 lanes to each row; TILE_LONG gives one row a
+// TILE_L1..TILE_L32 give 1..32 lanes to each row; TILE_MERGE splits the
+// tile's rows and entries evenly over the threads; TILE_LONG gives one row a
 // whole CTA.
 enum TileKind : int {
     TILE_L1 = 0, TILE_L2 = 1, TILE_L4 = 2, TILE_L8 = 3, TILE_L16 = 4, TILE_L32 = 5,
-    TILE_LONG = 6
+    TILE_LONG = 6,
+    TILE_MERGE = 7     // merge-path split of rows and entries over the CTA's threads
 };
 
 struct Tile {          // 16 bytes, read once per CTA

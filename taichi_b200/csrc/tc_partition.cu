@@ -31,6 +31,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "tc_internal.h"
@@ -834,8 +835,7 @@ static tc_status getsdf_device(int M, int N, const int *d_rowptr, const int *d_c
     TC_CUDA(cudaGetLastError());
     const size_t smem = sizeof(unsigned) * nw * 4;
     a.use_smem = smem <= 200 * 1024;
-    if (a.use_smem)
-        TC_CUDA(cudaFuncSetAttribute(morph_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (a.use_smem) TC_CHECK(ensure_smem((const void *)morph_kernel, smem));
     morph_kernel<<<1, 1024, a.use_smem ? smem : 0, s>>>(a);
     TC_CUDA(cudaGetLastError());
     ContourList cl;

@@ -57,9 +57,18 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, std::vector<Tile> &t
             ++r;
             continue;
         }
-        // candidate run: up to 1024 rows, stopping before a long row
+        // candidate run: up to 1024 rows (merge tiles: tile_rows), stopping
+        // before a long row
+        const int run_cap = prm.tile_mode == 0 ? std::min(rows_cap, kMergeRows) : 1024;
         int n = 0;
-        while (r + n < M && n < 1024 && rp[r + n + 1] - rp[r + n] <= long_len) ++n;
+        while (r + n < M && n < run_cap && rp[r + n + 1] - rp[r + n] <= long_len) ++n;
+        if (prm.tile_mode == 0) {          // merge tile: rows + entries split evenly
+            int rows = n;
+            while (rows > 1 && rp[r + rows] - rp[r] > kStageNnz) rows = (rows + 1) / 2;
+            tiles.push_back(Tile{r, rp[r], rp[r + rows] - rp[r], rows | (TILE_MERGE << 28)});
+            r += rows;
+            continue;
+        }
         int lanes = lanes_for((double)(rp[r + n] - rp[r]) / n, prm.max_lanes);
         int rows = std::min(std::min(n, tile_rows_for(lanes)), rows_cap);
         while (rows > 1 && rp[r + rows] - rp[r] > kStageNnz) rows = (rows + 1) / 2;   // fits a stage
@@ -329,15 +338,7 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
 {
     if (dp.ntiles <= 0) return TC_OK;
     const size_t smem = stream_smem_bytes(dp);
-    static size_t configured[2][64] = {};
-    int dev = 0;
-    TC_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return fail(TC_ERR_UNSUPPORTED, "device index %d", dev);
-    if (configured[SIGNED][dev] < smem) {
-        TC_CUDA(cudaFuncSetAttribute(spmv_tiles_kernel<SIGNED>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured[SIGNED][dev] = smem;
-    }
+    TC_CHECK(ensure_smem((const void *)spmv_tiles_kernel<SIGNED>, smem));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(dp.grid);
     cfg.blockDim = dim3(kBlock);
@@ -472,10 +473,8 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
         DevPlan tmp = p->dev_plan();
         const size_t smem = stream_smem_bytes(tmp);
         int per_sm = 0;
-        if (smem > 48 * 1024) {
-            TC_CUDA(cudaFuncSetAttribute(spmv_tiles_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            TC_CUDA(cudaFuncSetAttribute(spmv_tiles_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        }
+        TC_CHECK(ensure_smem((const void *)spmv_tiles_kernel<false>, smem));
+        TC_CHECK(ensure_smem((const void *)spmv_tiles_kernel<true>, smem));
         TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_tiles_kernel<true>, kBlock, smem));
         const int cps = std::max(1, std::min(per_sm, p->params.ctas_per_sm));
         p->grid = std::max(1, std::min(p->ntiles, cps * num_sms()));

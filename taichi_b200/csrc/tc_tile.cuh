@@ -167,56 +167,133 @@ __device__ __forceinline__ void tile_rows(const DevPlan &p, const Tile &t, const
         rows_pass<SIGNED, LANES>(p, t.row0, nr, base, src, x, y, wait);
 }
 
-// One lane per row: a thread owns up to kRPT consecutive rows and walks
-// their CSR words straight through (no lock-step rounds), after adding each
-// row's dense-diagonal terms.  Same per-row order as rows_pass.
+// Dense-diagonal terms of one row, offsets in order.
+__device__ __forceinline__ float diag_row(const DevPlan &p, const float *__restrict__ x, int r);
+
+// One lane per row, rows strided over the CTA (coalesced y and diagonal
+// loads): per row the diagonal terms in offset order, then the CSR words in
+// stored order -- the order of rows_pass<LANES = 1>.
 template <bool SIGNED, class Src>
-__device__ __forceinline__ void tile_rows1(const DevPlan &p, const Tile &t, const Src &src,
-                                           const float *__restrict__ x, float *__restrict__ y,
-                                           bool wait)
+__device__ __forceinline__ void tile_rows_seq(const DevPlan &p, const Tile &t, const Src &src,
+                                              const float *__restrict__ x, float *__restrict__ y,
+                                              bool wait)
 {
     const int nr = tile_nrows(t), row0 = t.row0;
-    for (int base = 0; base < nr; base += kBlock * kRPT) {
-        const int n = min(nr - base, kBlock * kRPT);
-        const int q = (n + kBlock - 1) / kBlock;            // rows per thread, 1..kRPT
-        const int lo = base + (int)threadIdx.x * q;
-        const int hi = min(lo + q, base + n);               // this thread's rows [lo, hi)
-        int e[kRPT + 1];
+    if (wait) wait_prior_grid();
+    for (int rl = threadIdx.x; rl < nr; rl += kBlock) {
+        const int b = src.row(rl), e = src.row(rl + 1);
+        float acc = p.dia_shapes > 0 ? diag_row(p, x, row0 + rl) : 0.f;
+#pragma unroll 2
+        for (int j = b; j < e; ++j) acc += gather<SIGNED>(x, src.word(j));
+        y[row0 + rl] = acc;
+    }
+}
+
+// ---------------------------------------------------------------- merge tile
+// Load-balanced walk of a tile (the merge-path split of Merrill & Garland):
+// the tile's nr row ends and nz CSR entries form one sequence of nr + nz
+// items, cut into equal runs of L = ceil((nr + nz) / kBlock) items, one run
+// per thread.  A thread finds where its run starts by a binary search on the
+// row pointers, gathers x for its run's entries eight at a time, and closes
+// the rows that end inside its run.  A row that starts in an earlier run
+// leaves a carry there; the thread that closes the row adds the carries of
+// the runs before it in thread order, so the sum order is fixed by the tile
+// alone.  Then each row gets its dense-diagonal terms and y is stored once.
+constexpr int kMergeRows = 2048;          // most rows in one merge tile
+constexpr int kMergeBatch = 8;            // gathers in flight per thread
+
+// Largest i in [0, nr] whose first CSR entry plus i does not pass item d.
+template <class Src>
+__device__ __forceinline__ int merge_split(const Src &src, int nr, int nz, int d)
+{
+    int lo = max(0, d - nz), hi = min(d, nr);
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (src.row(mid) + mid <= d) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Dense-diagonal terms of one row, offsets in order.
+__device__ __forceinline__ float diag_row(const DevPlan &p, const float *__restrict__ x, int r)
+{
+    float acc = 0.f;
+    if (r < p.row_start || r >= p.row_stop) return acc;
+    for (int s = 0; s < p.dia_shapes; ++s) {
+        const int4 sh = __ldg(p.shapes + s);
+        if (r < sh.x || r >= sh.y) continue;
+        const int2 dr = __ldg(p.shape_dias + s);
+        const int cb = r - sh.x + sh.z;
+        for (int d = dr.x; d < dr.y; ++d) {
+            const int c = cb + __ldg(p.offsets + d);
+            if (c >= sh.z && c < sh.z + sh.w) acc += __ldg(x + c);
+        }
+    }
+    return acc;
+}
+
+template <bool SIGNED, class Src>
+__device__ void tile_merge(const DevPlan &p, const Tile &t, const Src &src,
+                           const float *__restrict__ x, float *__restrict__ y, bool wait)
+{
+    __shared__ float rsum[kMergeRows];
+    __shared__ float carry[kBlock];
+    __shared__ int crow[kBlock];
+    const int nr = tile_nrows(t), nz = t.nnz, row0 = t.row0, tid = threadIdx.x;
+    const int total = nr + nz;
+    const int L = (total + kBlock - 1) / kBlock;
+    const int d0 = min(tid * L, total), d1 = min(d0 + L, total);
+    const int i0 = merge_split(src, nr, nz, d0);
+    int i1 = __shfl_down_sync(0xffffffffu, i0, 1);       // the next run starts where this ends
+    if ((tid & 31) == 31) i1 = merge_split(src, nr, nz, d1);
+    const int j0 = d0 - i0, j1 = d1 - i1;
+    if (wait) wait_prior_grid();
+    float acc = 0.f;
+    int r = i0;
+    int rend = r < nr ? src.row(r + 1) : nz;
+    for (int jb = j0; jb < j1; jb += kMergeBatch) {
+        float v[kMergeBatch];
 #pragma unroll
-        for (int k = 0; k <= kRPT; ++k) e[k] = lo < hi ? src.row(min(lo + k, hi)) : 0;
-        if (wait) wait_prior_grid();
-        float acc[kRPT];
+        for (int u = 0; u < kMergeBatch; ++u) {
+            const int j = jb + u;
+            v[u] = j < j1 ? gather<SIGNED>(x, src.word(j)) : 0.f;
+        }
 #pragma unroll
-        for (int k = 0; k < kRPT; ++k) acc[k] = 0.f;
-        if (p.dia_shapes > 0 && lo < hi && row0 + hi > p.row_start && row0 + lo < p.row_stop) {
-            for (int s = 0; s < p.dia_shapes; ++s) {
-                const int4 sh = __ldg(p.shapes + s);        // xStart, xStop, yStart, Msub
-                if (row0 + hi <= sh.x || row0 + lo >= sh.y) continue;
-                const int2 dr = __ldg(p.shape_dias + s);
-                const int cb = sh.z - sh.x;
-                for (int d = dr.x; d < dr.y; ++d) {
-                    const int off = __ldg(p.offsets + d);
-                    const int a = sh.x + max(0, -off), b = sh.y - max(0, off);
-                    float v[kRPT];
-#pragma unroll
-                    for (int k = 0; k < kRPT; ++k) {
-                        const int r = row0 + lo + k;
-                        v[k] = (lo + k < hi && r >= a && r < b) ? __ldg(x + r + cb + off) : 0.f;
-                    }
-#pragma unroll
-                    for (int k = 0; k < kRPT; ++k) acc[k] += v[k];
+        for (int u = 0; u < kMergeBatch; ++u) {
+            const int j = jb + u;
+            if (j < j1) {
+                while (j >= rend) {               // rows that end before entry j
+                    rsum[r] = acc;
+                    acc = 0.f;
+                    ++r;
+                    rend = src.row(r + 1);
                 }
+                acc += v[u];
             }
         }
-#pragma unroll
-        for (int k = 0; k < kRPT; ++k) {
-#pragma unroll 4
-            for (int j = e[k]; j < e[k + 1]; ++j) acc[k] += gather<SIGNED>(x, src.word(j));
-        }
-#pragma unroll
-        for (int k = 0; k < kRPT; ++k)
-            if (lo + k < hi) y[row0 + lo + k] = acc[k];
     }
+    while (r < i1) {                              // rows ending at the end of the run
+        rsum[r] = acc;
+        acc = 0.f;
+        ++r;
+    }
+    const bool partial = r < nr && j1 > max(j0, r < nr ? src.row(r) : nz);
+    crow[tid] = partial ? r : -1;
+    carry[tid] = acc;
+    __syncthreads();
+    if (i1 > i0 && tid > 0 && crow[tid - 1] == i0) {   // row i0 began in earlier runs
+        float add = 0.f;
+        for (int u = tid - 1; u >= 0 && crow[u] == i0; --u) add += carry[u];
+        rsum[i0] += add;
+    }
+    __syncthreads();
+    for (int rr = tid; rr < nr; rr += kBlock) {
+        float v = rsum[rr];
+        if (p.dia_shapes > 0) v += diag_row(p, x, row0 + rr);
+        y[row0 + rr] = v;
+    }
+    __syncthreads();                              // rsum / carry are reused by the next tile
 }
 
 // One row with more entries than the planner's per-tile limit: the whole CTA
@@ -272,7 +349,8 @@ __device__ __forceinline__ void run_tile_src(const DevPlan &p, const Tile &t, co
                                              bool wait)
 {
     switch (tile_kind(t)) {
-    case TILE_L1: tile_rows1<SIGNED>(p, t, src, x, y, wait); break;
+    case TILE_MERGE: tile_merge<SIGNED>(p, t, src, x, y, wait); break;
+    case TILE_L1: tile_rows_seq<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_L2: tile_rows<SIGNED, 2>(p, t, src, x, y, wait); break;
     case TILE_L4: tile_rows<SIGNED, 4>(p, t, src, x, y, wait); break;
     case TILE_L8: tile_rows<SIGNED, 8>(p, t, src, x, y, wait); break;

@@ -146,18 +146,18 @@ extern "C" tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const
         f.xStop = best_plan->h_xStop.data(); f.nDiasPtr = best_plan->h_nDiasPtr.data();
         f.neg_offsets = best_plan->h_offsets.data();
         f.csrRow = rp.data(); f.csrCol = cw.data();
-        const int rows_c[] = {256, 512, 1024, 2048};
-        const int lanes_c[] = {32, 8};
-        const int cps_c[] = {4, 2, 8};
-        for (int cps : cps_c)
-            for (int lanes : lanes_c)
-                for (int rows : rows_c) {
+        // {tile_mode, tile_rows, max_lanes, ctas_per_sm}, most promising first
+        const int cand[][4] = {{0, 512, 32, 4}, {0, 2048, 32, 4}, {0, 256, 32, 4}, {0, 1024, 32, 2},
+                               {0, 1024, 32, 8}, {0, 512, 32, 8}, {0, 2048, 32, 2}, {1, 1024, 32, 4},
+                               {1, 1024, 8, 4}, {0, 256, 32, 8}, {1, 1024, 32, 2}, {0, 512, 32, 2}};
+        for (const auto &cnd : cand) {
                     if (st != TC_OK || trials >= max_trials) break;
                     tc_params q = best.params;
-                    q.tile_rows = rows; q.max_lanes = lanes; q.ctas_per_sm = cps;
+                    q.tile_mode = cnd[0]; q.tile_rows = cnd[1]; q.max_lanes = cnd[2];
+                    q.ctas_per_sm = cnd[3];
                     q.flags &= ~TC_FLAG_KEEP_HOST;
-                    if (q.tile_rows == best.params.tile_rows && q.max_lanes == best.params.max_lanes &&
-                        q.ctas_per_sm == best.params.ctas_per_sm)
+                    if (q.tile_mode == best.params.tile_mode && q.tile_rows == best.params.tile_rows &&
+                        q.max_lanes == best.params.max_lanes && q.ctas_per_sm == best.params.ctas_per_sm)
                         continue;
                     tc_plan *p = nullptr;
                     st = tc_plan_from_format(M, N, &f, &q, stream, &p);

@@ -39,8 +39,8 @@ def test_served_results_identical_to_solo(tc, dev, mode):
     rng = np.random.default_rng(3 + mode)
     n = 300
     matrix = rng.integers(0, len(plans), n)
-    # bursts: many requests arrive together, so batches mix matrices
-    arrival = np.sort(rng.uniform(0, 0.02, n))
+    # a burst: the requests arrive within half a millisecond, so batches mix matrices
+    arrival = np.sort(rng.uniform(0, 0.0005, n))
     xs, ys, want = [], [], []
     for r in range(n):
         M, N, rp, col = mats[matrix[r]]
