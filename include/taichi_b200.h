@@ -159,6 +159,23 @@ TC_API tc_status tc_getsdf(int M, int N, const int *d_rowptr, const int *d_col, 
                     int *mF, int *W, int *corners, int max_corners, int *ncorners,
                     unsigned char *stages, void *stream);
 
+/* The thumbnail stages of tc_getsdf (raster, filled, open-open, subtracted,
+ * eye-opened; 5 x height x W bytes, 0/255) written to caller-owned DEVICE
+ * memory, without allocating anything.  No counterpart in the reference: it
+ * is for callers that cannot call cudaMalloc at this point -- code running
+ * while another framework owns the device allocator, or a latency-critical
+ * path that must not add cudaMalloc/cudaFree (they synchronize the device).
+ * The working images live in a fixed device array of the library (512 KB,
+ * held on every GPU that loads the library until exit), so the thumbnail is
+ * limited to height <= 512 and W <= 1024 (TC_ERR_CAPACITY beyond).  The first
+ * call on a device looks up that array's address; make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race.  *W
+ * receives the width (0 when the matrix is too small for a thumbnail, in
+ * which case nothing is written).  Synchronizes `stream`. */
+TC_API tc_status tc_thumbnail_noalloc(int M, int N, const int *d_rowptr, const int *d_col,
+                                      const tc_params *p, unsigned char *d_stages, int *W,
+                                      void *stream);
+
 /* Border following (findContours RETR_CCOMP / CHAIN_APPROX_NONE order) of a
  * host H x W 0/nonzero image on the GPU.  Writes contour lengths (up to
  * max_contours) and, for each, its first point and middle point (4 ints) to

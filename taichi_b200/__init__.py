@@ -60,7 +60,7 @@ EXPORTS = (
     "tc_trace_contours", "tc_read_mtx", "tc_free", "tc_batch_create", "tc_batch_run",
     "tc_batch_graph_launch", "tc_batch_destroy", "tc_tune", "tc_tune_cache_clear",
     "tc_serve_config_default", "tc_server_create", "tc_server_admit", "tc_server_evict",
-    "tc_server_hbm_used", "tc_server_run", "tc_server_destroy",
+    "tc_server_hbm_used", "tc_server_run", "tc_server_destroy", "tc_thumbnail_noalloc",
 )
 
 
@@ -97,6 +97,8 @@ def lib():
         L.tc_getsdf.argtypes = [C.c_int, C.c_int, vp, vp, C.POINTER(Params), _IP, _IP, vp,
                                 C.c_int, _IP, vp, vp]
         L.tc_trace_contours.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, _IP]
+        L.tc_thumbnail_noalloc.argtypes = [C.c_int, C.c_int, vp, vp, C.POINTER(Params), vp,
+                                           _IP, vp]
         L.tc_read_mtx.argtypes = [C.c_char_p, _IP, _IP, C.POINTER(C.c_int64), C.POINTER(_IP),
                                   C.POINTER(_IP), C.POINTER(C.POINTER(C.c_float)), _IP]
         L.tc_free.argtypes = [vp]

@@ -1178,3 +1178,107 @@ extern "C" tc_status tc_trace_contours(const unsigned char *img, int H, int W, i
     }
     return n > max_contours ? fail(TC_ERR_CAPACITY, "%d contours, room for %d", n, max_contours) : TC_OK;
 }
+
+// ======================================================================
+// Thumbnail stages without any allocation
+// ======================================================================
+// Some callers cannot allocate device memory at the point where they need
+// the partitioner's thumbnail: code running while another framework owns the
+// device allocator, or a caller that must not add cudaMalloc/cudaFree (which
+// synchronize the device) to a latency-critical path.  This variant of the
+// raster + morphology stages takes its scratch -- the eight bit-packed
+// working images and a status word -- from the fixed array below instead of
+// cudaMalloc.  The array holds at most a 512 x 1024 thumbnail (512 KB); it
+// lives on every GPU that loads the library until the process exits.
+namespace tc {
+namespace {
+
+constexpr int kNoAllocMaxH = 512, kNoAllocMaxW = 1024;
+constexpr int kNoAllocWords = 8 * kNoAllocMaxH * (kNoAllocMaxW / 32);
+static __device__ __align__(256) unsigned g_thumb_scratch[kNoAllocWords + 64];
+
+std::mutex g_noalloc_mu;
+unsigned *g_noalloc_addr[64] = {};
+
+// Device address of g_thumb_scratch on the current device (looked up once per
+// device; the host-side name is not a device address).
+tc_status noalloc_scratch(unsigned **out)
+{
+    int dev = 0;
+    TC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(TC_ERR_UNSUPPORTED, "device index %d", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_thumb_scratch);
+        if (e != cudaSuccess)
+            return fail(TC_ERR_CUDA, "cudaGetSymbolAddress(thumbnail scratch): %s", cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<unsigned *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return TC_OK;
+}
+
+}  // namespace
+}  // namespace tc
+
+// Same images as tc_getsdf's `stages`, written to caller-owned device memory;
+// allocates nothing.  The first call on a device looks up the scratch array's
+// address (make it before any stream capture).  All calls share that array,
+// so calls that overlap on the GPU (other streams, other threads) race; each
+// call rewrites every word it reads before reading it and clears the status
+// word itself.  Synchronizes `stream` to read the status word.
+extern "C" tc_status tc_thumbnail_noalloc(int M, int N, const int *d_rowptr, const int *d_col,
+                                          const tc_params *params, unsigned char *d_stages, int *W_out,
+                                          void *stream)
+{
+    if (!W_out || M < 0 || N < 0 || (M > 0 && !d_rowptr)) return tc::fail(TC_ERR_INVALID, "tc_thumbnail_noalloc: bad arguments");
+    *W_out = 0;
+    tc_params p;
+    tc_params_default(&p);
+    if (params) p = *params;
+    const int H = p.thumb_height;
+    if (M <= H) return TC_OK;                      // no thumbnail (morohutils.cu:192-196)
+    const int W = (int)((double)H / (double)M * N);
+    if (W <= 0) return tc::fail(TC_ERR_UNSUPPORTED, "thumbnail width is 0 (N < M/%d)", H);
+    if (H > tc::kNoAllocMaxH || W > tc::kNoAllocMaxW)
+        return tc::fail(TC_ERR_CAPACITY, "thumbnail %d x %d exceeds the fixed scratch (%d x %d)", H, W,
+                        tc::kNoAllocMaxH, tc::kNoAllocMaxW);
+    if (!d_stages || !d_col) return tc::fail(TC_ERR_INVALID, "tc_thumbnail_noalloc: null buffer");
+    unsigned *scratch = nullptr;
+    TC_CHECK(tc::noalloc_scratch(&scratch));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int pM = M / H, pN = N / W, WW = (W + 31) / 32;
+    const size_t nw = (size_t)H * WW;
+    auto img = [&](int k) { return tc::Img{scratch + k * nw, H, W, WW}; };
+    int *flag = reinterpret_cast<int *>(scratch + tc::kNoAllocWords);
+    TC_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+    tc::MorphArgs a;
+    a.B = img(0); a.F = img(1); a.O2 = img(2); a.D = img(3); a.E = img(4);
+    a.T1 = img(5); a.T2 = img(6); a.T3 = img(7);
+    a.open_len = p.open_len;
+    a.eye = p.eye_size;
+    a.flag = flag;
+    tc::raster_kernel<<<H, 256, sizeof(unsigned) * WW, s>>>(d_rowptr, d_col, M, pM, pN, a.B);
+    TC_CUDA(cudaGetLastError());
+    const size_t smem = sizeof(unsigned) * nw * 4;
+    a.use_smem = smem <= 200 * 1024;
+    if (a.use_smem) {   // raise (never lower) the kernel's shared-memory limit
+        cudaFuncAttributes fa;
+        TC_CUDA(cudaFuncGetAttributes(&fa, tc::morph_kernel));
+        if ((size_t)fa.maxDynamicSharedSizeBytes < smem)
+            TC_CUDA(cudaFuncSetAttribute(tc::morph_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    tc::morph_kernel<<<1, 1024, a.use_smem ? smem : 0, s>>>(a);
+    TC_CUDA(cudaGetLastError());
+    const size_t px = (size_t)H * W;
+    for (int k = 0; k < 5; ++k)
+        tc::unpack_kernel<<<tc::cdiv((long)px, 256), 256, 0, s>>>(img(k), d_stages + k * px);
+    TC_CUDA(cudaGetLastError());
+    int hflag = 0;
+    TC_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TC_CUDA(cudaStreamSynchronize(s));
+    if (hflag) return tc::fail(TC_ERR_UNSUPPORTED, "hole fill did not converge");
+    *W_out = W;
+    return TC_OK;
+}
