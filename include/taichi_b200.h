@@ -56,7 +56,9 @@ typedef struct tc_params {
     int ctas_per_sm;      /* resident CTAs per SM of the multiply grid (4)     */
     int tile_mode;        /* 0: rows and entries split evenly over a CTA's
                              threads (merge path); 1: lanes per row chosen
-                             from the tile's row lengths (1)                   */
+                             from the tile's row lengths; 2: stream tiles
+                             (entry-parallel gather into shared memory, then
+                             row sums), one CTA per tile (1)                   */
     int flags;            /* TC_FLAG_*                                         */
 } tc_params;
 
@@ -65,6 +67,8 @@ typedef struct tc_params {
 #define TC_FLAG_NO_PDL       0x4  /* launch without programmatic dependent
                                      launch (the multiply then starts only
                                      when the previous kernel has finished)  */
+#define TC_FLAG_ROWS_STRIDED 0x8  /* stream tiles (tile_mode 2) sum one row
+                                     per thread, never 4 consecutive rows   */
 
 TC_API void tc_params_default(tc_params *p);
 
@@ -274,8 +278,13 @@ TC_API int64_t tc_server_hbm_used(const tc_server *s);
  * seconds after the call starts (non-decreasing), multiplies matrix[r] by the
  * host vector h_x[r] and leaves y in h_y[r] (pinned host memory gives full
  * copy bandwidth).  mode 0: continuous batching; mode 1: one synchronous
- * request at a time (the plain form).  latency_ms[r] (optional) receives
- * completion minus arrival. */
+ * request at a time (the plain form).  With TC_SERVE_DEVICE_VECTORS added to
+ * the mode, h_x[r] / h_y[r] are device vectors owned by the caller: nothing is
+ * copied, a batch is one launch over its requests' tiles and the plain form
+ * is one synchronous tc_spmv per request (requests in flight together must
+ * not share a y).  latency_ms[r] (optional) receives completion minus
+ * arrival. */
+#define TC_SERVE_DEVICE_VECTORS 2
 TC_API tc_status tc_server_run(tc_server *s, int nreq, const double *arrival_s, const int *matrix,
                                const float *const *h_x, float *const *h_y, int mode,
                                double *latency_ms, tc_serve_stats *stats);

@@ -19,6 +19,7 @@ _LIB = None
 TC_FLAG_NO_PARTITION = 0x1
 TC_FLAG_KEEP_HOST = 0x2
 TC_FLAG_NO_PDL = 0x4
+TC_FLAG_ROWS_STRIDED = 0x8
 
 _IP = C.POINTER(C.c_int)
 
@@ -175,6 +176,9 @@ class ServeStats(C.Structure):
                 ("mean_ms", C.c_double), ("max_ms", C.c_double), ("mean_batch", C.c_double)]
 
 
+SERVE_DEVICE_VECTORS = 2     # tc_server_run mode bit: requests carry device x / y
+
+
 class Server:
     """Resident matrices + continuous batching of SpMV requests (tc_server)."""
 
@@ -202,7 +206,8 @@ class Server:
         return lib().tc_server_hbm_used(self._h)
 
     def run(self, arrival_s, matrix, xs, ys, mode=0):
-        """xs / ys: per-request host arrays (numpy, float32, contiguous).
+        """xs / ys: per-request host arrays (numpy or pinned torch, float32,
+        contiguous); device tensors with mode | SERVE_DEVICE_VECTORS.
         Returns (stats dict, latency_ms array)."""
         n = len(matrix)
         arr = np.ascontiguousarray(arrival_s, np.float64)

@@ -80,8 +80,8 @@ static tc_status check_params(const tc_params &p)
     if (p.tile_rows < 1 || p.tile_rows > tc::kMaxTileRows)
         return fail(TC_ERR_INVALID, "tile_rows %d outside [1, %d]", p.tile_rows, tc::kMaxTileRows);
     if (p.tile_nnz < 1) return fail(TC_ERR_INVALID, "tile_nnz %d < 1", p.tile_nnz);
-    if (p.tile_mode < 0 || p.tile_mode > 1)
-        return fail(TC_ERR_INVALID, "tile_mode %d is not 0 or 1", p.tile_mode);
+    if (p.tile_mode < 0 || p.tile_mode > 2)
+        return fail(TC_ERR_INVALID, "tile_mode %d is not 0, 1 or 2", p.tile_mode);
     if (p.ctas_per_sm < 1 || p.ctas_per_sm > 32)
         return fail(TC_ERR_INVALID, "ctas_per_sm %d outside [1, 32]", p.ctas_per_sm);
     if (p.max_lanes < 1 || p.max_lanes > 32 || (p.max_lanes & (p.max_lanes - 1)))
@@ -132,6 +132,11 @@ tc_status tc_plan_from_format(int M, int N, const tc_format *f, const tc_params 
             delete p;
             return fail(TC_ERR_FORMAT, "nDiasPtr does not span neg_offsets");
         }
+        for (int s = 0; s < f->dia_shapes; ++s)
+            if (f->nDiasPtr[s + 1] < f->nDiasPtr[s]) {
+                delete p;
+                return fail(TC_ERR_FORMAT, "nDiasPtr decreases at shape %d", s);
+            }
     }
     std::vector<int> zero_rp;
     const int *rp = f->csrRow;

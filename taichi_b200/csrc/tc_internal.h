@@ -41,27 +41,43 @@ tc_status ensure_smem(const void *kernel, size_t bytes);
 // ------------------------------------------------------------- tile plan
 // A multiply tile is a run of consecutive rows processed by one CTA.  Kinds
 // TILE_L1..TILE_L32 give 1..32 lanes to each row; TILE_MERGE splits the
-// tile's rows and entries evenly over the threads; TILE_LONG gives one row a
-// whole CTA.
+// tile's rows and entries evenly over the threads; TILE_STREAM gathers every
+// entry's x term into shared memory with coalesced word loads, then sums each
+// row there; TILE_LONG gives one row a whole CTA.
 enum TileKind : int {
     TILE_L1 = 0, TILE_L2 = 1, TILE_L4 = 2, TILE_L8 = 3, TILE_L16 = 4, TILE_L32 = 5,
     TILE_LONG = 6,
-    TILE_MERGE = 7     // merge-path split of rows and entries over the CTA's threads
+    TILE_MERGE = 7,    // merge-path split of rows and entries over the CTA's threads
+    TILE_STREAM = 8,   // entry-parallel gather, then row-parallel sums in shared memory
+    TILE_STREAM4 = 9   // the same with 4 consecutive rows per thread (row0 % 4 == 0)
 };
 
 struct Tile {          // 16 bytes, read once per CTA
     int row0;          // first row
     int nz0;           // first CSR entry (rowptr[row0])
     int nnz;           // CSR entries of the tile
-    int nrows_kind;    // nrows | kind << 28
+    int nrows_kind;    // nrows (bits 0-11) | diagonal class << 12 (16 bits) | kind << 28
 };
 
-__host__ __device__ inline int tile_nrows(const Tile &t) { return t.nrows_kind & 0x0fffffff; }
+// Diagonal class of a tile: how its rows meet the dense-diagonal shapes.
+constexpr int kDiagGeneral = 0;        // per-row search over the shapes
+constexpr int kDiagNone = 0xffff;      // no row of the tile is in any shape
+// otherwise s + 1: every row lies in shape s alone and every offset of s
+// lands inside the shape's columns for every row of the tile
+constexpr int kMaxTileNrows = 0xfff;
+
+__host__ __device__ inline int tile_nrows(const Tile &t) { return t.nrows_kind & 0xfff; }
+__host__ __device__ inline int tile_dclass(const Tile &t) { return (t.nrows_kind >> 12) & 0xffff; }
 __host__ __device__ inline int tile_kind(const Tile &t) { return (t.nrows_kind >> 28) & 0xf; }
+__host__ __device__ inline int tile_word(int nrows, int kind) { return nrows | (kind << 28); }
 
 constexpr int kBlock = 256;           // threads per CTA of the multiply kernels
 constexpr int kMaxTileRows = 1 << 20; // planner limit on rows per tile
 constexpr int kStageNnz = 8192;       // CSR words of a tile staged in shared memory
+constexpr int kStreamNnz = 4096;      // most entries of a TILE_STREAM tile
+constexpr int kStreamRows = 1024;     // most rows of a TILE_STREAM tile (4 per thread)
+constexpr int kStreamRowMax = 128;    // longer rows leave stream tiles for lane tiles
+constexpr int kStream4Rows = 1024;    // most rows of a TILE_STREAM4 tile (a run of 4 per thread)
 
 // Everything a multiply kernel needs about one plan (passed by value).
 struct DevPlan {
@@ -76,6 +92,8 @@ struct DevPlan {
     int pdl;                // launch with programmatic stream serialization
     int stage_rp, stage_cw; // ints per shared-memory stage (row pointers, CSR words)
     int grid;               // persistent grid size
+    int per_tile;           // one CTA per tile (stream plans): 1, or 2 when only stream
+                            // and long tiles occur (the lean kernel)
     int *err;               // device error word (1: a bounded wait gave up)
 };
 
@@ -100,6 +118,7 @@ struct tc_plan {
     int4 *d_shapes = nullptr;
     int2 *d_shape_dias = nullptr;
     int ntiles = 0, ntiles_vector = 0, ntiles_long = 0;
+    int ntiles_lanes = 0;                // lane and merge tiles (TILE_L1..L32, TILE_MERGE)
     int max_span = 0;
     int stage_rp = 8, stage_cw = 8, grid = 1;
     int *d_err = nullptr;
@@ -124,8 +143,14 @@ namespace tc {
 tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol,
                       cudaStream_t stream);
 // Host tile planner (row-length histogram -> tile kinds).
-void plan_tiles(const int *rowptr, int M, const tc_params &prm, std::vector<Tile> &tiles,
-                int *nvec, int *nlong);
+// Stream tiles hold at most nnz_csr / min_tiles entries (not below 512), so
+// a small matrix still spreads over the GPU.
+void plan_tiles(const int *rowptr, int M, const tc_params &prm, int min_tiles,
+                std::vector<Tile> &tiles, int *nvec, int *nlong);
+// Resident CTAs per SM the lean one-CTA-per-tile kernel is compiled for
+// (40 registers: the stream tiles' words, terms and row pointers fit
+// without spills).
+constexpr int kLeanMinBlocks = 6, kLeanMinBlocksSigned = 6;
 // Launch of the multiply kernel for one plan.
 tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
 tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,

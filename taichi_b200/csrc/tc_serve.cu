@@ -11,7 +11,9 @@
 // matrices, the same tile code as tc_spmv, so each y is bit-identical alone
 // and in a mix), and the y copies go on the context's stream.  Several
 // contexts are in flight at once, so one batch's copies overlap another's
-// multiply.  The plain form multiplies one request at a time.
+// multiply.  The plain form multiplies one request at a time.  With
+// TC_SERVE_DEVICE_VECTORS the requests' x and y are device vectors that the
+// caller owns (no copies; a batch is one launch over the requests' tiles).
 
 #include <cuda_runtime.h>
 
@@ -198,20 +200,26 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
     for (int r = 0; r < nreq; ++r)
         if (matrix[r] < 0 || matrix[r] >= (int)sv->plans.size() || !sv->plans[matrix[r]])
             return fail(TC_ERR_INVALID, "request %d names matrix %d, which is not admitted", r, matrix[r]);
+    if (mode < 0 || mode > 3) return fail(TC_ERR_INVALID, "tc_server_run: mode %d", mode);
+    const bool device_vectors = (mode & TC_SERVE_DEVICE_VECTORS) != 0;
     std::vector<double> done(nreq, 0.0);
     int64_t batches = 0, launched = 0;
     const double t0 = tc::now_s();
     auto slot_floats = [](int64_t n) { return ((n + 63) / 64) * 64; };   // 256-byte slots
 
-    if (mode == 1) {   // plain: one synchronous request at a time
+    if (mode & 1) {    // plain: one synchronous request at a time
         tc_server::Ctx &c = sv->ctx[0];
         for (int r = 0; r < nreq; ++r) {
             while (tc::now_s() - t0 < arrival_s[r]) { }
             const tc_plan *p = sv->plans[matrix[r]];
-            float *dx = c.arena, *dy = c.arena + slot_floats(p->N);
-            if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x[r], 4 * (size_t)p->N, cudaMemcpyHostToDevice, c.s));
-            TC_CHECK(tc_spmv(p, dx, dy, c.s));
-            if (p->M) TC_CUDA(cudaMemcpyAsync(h_y[r], dy, 4 * (size_t)p->M, cudaMemcpyDeviceToHost, c.s));
+            if (device_vectors) {
+                TC_CHECK(tc_spmv(p, h_x[r], h_y[r], c.s));
+            } else {
+                float *dx = c.arena, *dy = c.arena + slot_floats(p->N);
+                if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x[r], 4 * (size_t)p->N, cudaMemcpyHostToDevice, c.s));
+                TC_CHECK(tc_spmv(p, dx, dy, c.s));
+                if (p->M) TC_CUDA(cudaMemcpyAsync(h_y[r], dy, 4 * (size_t)p->M, cudaMemcpyDeviceToHost, c.s));
+            }
             TC_CUDA(cudaStreamSynchronize(c.s));
             done[r] = tc::now_s() - t0;
             ++batches;
@@ -246,16 +254,20 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
             while (!pending.empty() && nb < sv->cfg.max_batch) {
                 const int r = pending.front();
                 const tc_plan *p = sv->plans[matrix[r]];
-                const int64_t need = slot_floats(p->N) + slot_floats(p->M);
-                if ((used + need) * 4 > sv->cfg.arena_bytes) break;
-                float *dx = c.arena + used, *dy = dx + slot_floats(p->N);
-                used += need;
-                c.h_desc[nb] = tc::ReqDesc{matrix[r], tiles, dx, dy};
+                if (device_vectors) {   // the request's own device x and y
+                    c.h_desc[nb] = tc::ReqDesc{matrix[r], tiles, h_x[r], h_y[r]};
+                } else {                // x and y slots in the context's arena
+                    const int64_t need = slot_floats(p->N) + slot_floats(p->M);
+                    if ((used + need) * 4 > sv->cfg.arena_bytes) break;
+                    float *dx = c.arena + used, *dy = dx + slot_floats(p->N);
+                    used += need;
+                    c.h_desc[nb] = tc::ReqDesc{matrix[r], tiles, dx, dy};
+                    if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x[r], 4 * (size_t)p->N, cudaMemcpyHostToDevice, c.s));
+                }
                 tiles += p->ntiles;
                 c.reqs.push_back(r);
                 pending.pop_front();
                 ++nb;
-                if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x[r], 4 * (size_t)p->N, cudaMemcpyHostToDevice, c.s));
             }
             TC_CUDA(cudaMemcpyAsync(c.d_desc, c.h_desc, sizeof(tc::ReqDesc) * nb, cudaMemcpyHostToDevice, c.s));
             if (tiles > 0) {
@@ -263,7 +275,7 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
                 tc::serve_kernel<<<grid, tc::kBlock, 0, c.s>>>(sv->d_plans, c.d_desc, nb, tiles);
                 TC_CUDA(cudaGetLastError());
             }
-            for (int i = 0; i < nb; ++i) {
+            for (int i = 0; i < nb && !device_vectors; ++i) {
                 const int r = c.reqs[i];
                 const tc_plan *p = sv->plans[matrix[r]];
                 if (p->M) TC_CUDA(cudaMemcpyAsync(h_y[r], c.h_desc[i].y, 4 * (size_t)p->M, cudaMemcpyDeviceToHost, c.s));

@@ -42,9 +42,10 @@ static int kind_of(int lanes)
     return k;
 }
 
-void plan_tiles(const int *rp, int M, const tc_params &prm, std::vector<Tile> &tiles, int *nvec,
-                int *nlong)
+void plan_tiles(const int *rp, int M, const tc_params &prm, int min_tiles, std::vector<Tile> &tiles,
+                int *nvec, int *nlong)
 {
+    const int spread = (int)std::min<int64_t>(kStreamNnz, std::max<int64_t>(512, (int64_t)rp[M] / std::max(1, min_tiles)));
     const int long_len = std::max(1, std::min(prm.tile_nnz, kStageNnz));
     const int rows_cap = std::max(1, std::min(prm.tile_rows, kMaxTileRows));
     tiles.clear();
@@ -52,20 +53,45 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, std::vector<Tile> &t
     int r = 0;
     while (r < M) {
         if (rp[r + 1] - rp[r] > long_len) {
-            tiles.push_back(Tile{r, rp[r], rp[r + 1] - rp[r], 1 | (TILE_LONG << 28)});
+            tiles.push_back(Tile{r, rp[r], rp[r + 1] - rp[r], tile_word(1, TILE_LONG)});
             ++*nlong;
             ++r;
             continue;
         }
+        if (prm.tile_mode == 2 && rp[r + 1] - rp[r] <= kStreamRowMax) {
+            // stream tile: short rows up to the row and entry caps; a tile
+            // that starts on a multiple of 4 rows and holds many rows runs 4
+            // consecutive rows per thread (TILE_STREAM4)
+            const bool a4 = (r & 3) == 0 && !(prm.flags & TC_FLAG_ROWS_STRIDED);
+            const int cap_rows = std::min(rows_cap, a4 ? kStream4Rows : kStreamRows);
+            const int cap_nnz = std::max(1, std::min(2 * prm.tile_nnz, spread));
+            int n = 0;
+            while (r + n < M && n < cap_rows && rp[r + n + 1] - rp[r + n] <= kStreamRowMax &&
+                   rp[r + n + 1] - rp[r] <= cap_nnz)
+                ++n;
+            if (n == 0) n = 1;        // a single row longer than cap_nnz but <= kStreamRowMax
+            const bool four = a4 && n >= 2 * kBlock;
+            if (!four) n = std::min(n, kStreamRows);
+            if (r + n < M) {          // end on a multiple of 256 rows (whole row sweeps), else of 4
+                const int cut = (r + n) & ~255;
+                if (cut - r >= 256) n = cut - r;
+                else if (n > 4) n -= (r + n) & 3;
+            }
+            tiles.push_back(Tile{r, rp[r], rp[r + n] - rp[r], tile_word(n, four ? TILE_STREAM4 : TILE_STREAM)});
+            r += n;
+            continue;
+        }
         // candidate run: up to 1024 rows (merge tiles: tile_rows), stopping
-        // before a long row
+        // before a long row (stream mode: before a short row too)
         const int run_cap = prm.tile_mode == 0 ? std::min(rows_cap, kMergeRows) : 1024;
         int n = 0;
-        while (r + n < M && n < run_cap && rp[r + n + 1] - rp[r + n] <= long_len) ++n;
+        while (r + n < M && n < run_cap && rp[r + n + 1] - rp[r + n] <= long_len &&
+               !(prm.tile_mode == 2 && rp[r + n + 1] - rp[r + n] <= kStreamRowMax))
+            ++n;
         if (prm.tile_mode == 0) {          // merge tile: rows + entries split evenly
             int rows = n;
             while (rows > 1 && rp[r + rows] - rp[r] > kStageNnz) rows = (rows + 1) / 2;
-            tiles.push_back(Tile{r, rp[r], rp[r + rows] - rp[r], rows | (TILE_MERGE << 28)});
+            tiles.push_back(Tile{r, rp[r], rp[r + rows] - rp[r], tile_word(rows, TILE_MERGE)});
             r += rows;
             continue;
         }
@@ -74,7 +100,7 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, std::vector<Tile> &t
         while (rows > 1 && rp[r + rows] - rp[r] > kStageNnz) rows = (rows + 1) / 2;   // fits a stage
         lanes = lanes_for((double)(rp[r + rows] - rp[r]) / rows, prm.max_lanes);
         if (lanes > 1) ++*nvec;
-        tiles.push_back(Tile{r, rp[r], rp[r + rows] - rp[r], rows | (kind_of(lanes) << 28)});
+        tiles.push_back(Tile{r, rp[r], rp[r + rows] - rp[r], tile_word(rows, kind_of(lanes))});
         r += rows;
     }
 }
@@ -147,7 +173,7 @@ __device__ __forceinline__ void stage_tile(const DevPlan &p, int t, int *rp_buf,
 {
     if (t >= p.ntiles) return;
     const Tile tile = p.tiles[t];
-    if (tile_kind(tile) == TILE_LONG) return;
+    if (tile_kind(tile) == TILE_LONG || tile_kind(tile) >= TILE_STREAM) return;   // read from global
     const Window wr = window_of(tile.row0, (long)tile.row0 + tile_nrows(tile) + 1);
     const Window wc = window_of(tile.nz0, (long)tile.nz0 + tile.nnz);
     const unsigned br = (unsigned)(wr.b - wr.a), bc = tile.nnz ? (unsigned)(wc.b - wc.a) : 0u;
@@ -188,7 +214,7 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
         int *const rp_s = buf + s * stride;
         int *const cw_s = rp_s + p.stage_rp;
         const Tile tile = p.tiles[t];
-        if (tile_kind(tile) == TILE_LONG) {
+        if (tile_kind(tile) == TILE_LONG || tile_kind(tile) >= TILE_STREAM) {
             run_tile<SIGNED>(p, tile, x, y, !waited);
         } else {
             const bool ok = mbar_wait(bar + s, (phases >> s) & 1u);
@@ -210,6 +236,27 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
         }
     }
     if (!waited) wait_prior_grid();
+}
+
+// The multiply of a stream plan: one CTA per tile, no shared-memory stages
+// (stream tiles read their CSR words as coalesced int4s; lane and long tiles
+// read global memory directly).  LEAN: the plan holds only stream and long
+// tiles, so the kernel carries no lane-tile code and fits more CTAs per SM.
+template <bool SIGNED, bool LEAN>
+__global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned : kLeanMinBlocks) : 1)
+    spmv_grid_kernel(DevPlan p, const float *__restrict__ x, float *__restrict__ y)
+{
+    allow_next_grid();
+    const Tile t = p.tiles[blockIdx.x];
+    if (LEAN) {
+        switch (tile_kind(t)) {
+        case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, true); break;
+        case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, true); break;
+        default: long_row<SIGNED>(p, t, x, y, true); break;
+        }
+    } else {
+        run_tile<SIGNED>(p, t, x, y, true);
+    }
 }
 
 // SpMM: a warp owns kRPW consecutive rows at a time; lane l holds columns
@@ -337,10 +384,10 @@ template <bool SIGNED>
 static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaStream_t s)
 {
     if (dp.ntiles <= 0) return TC_OK;
-    const size_t smem = stream_smem_bytes(dp);
-    TC_CHECK(ensure_smem((const void *)spmv_tiles_kernel<SIGNED>, smem));
+    const size_t smem = dp.per_tile ? 0 : stream_smem_bytes(dp);
+    if (!dp.per_tile) TC_CHECK(ensure_smem((const void *)spmv_tiles_kernel<SIGNED>, smem));
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(dp.grid);
+    cfg.gridDim = dim3(dp.per_tile ? dp.ntiles : dp.grid);
     cfg.blockDim = dim3(kBlock);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -349,7 +396,9 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
     attr[0].val.programmaticStreamSerializationAllowed = dp.pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_tiles_kernel<SIGNED>, dp, x, y));
+    if (dp.per_tile == 2) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, true>, dp, x, y));
+    else if (dp.per_tile) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, false>, dp, x, y));
+    else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_tiles_kernel<SIGNED>, dp, x, y));
     return TC_OK;
 }
 
@@ -400,6 +449,7 @@ tc::DevPlan tc_plan::dev_plan() const
     d.stage_rp = stage_rp;
     d.stage_cw = stage_cw;
     d.grid = grid;
+    d.per_tile = params.tile_mode != 2 ? 0 : (ntiles_lanes == 0 ? 2 : 1);
     d.err = d_err;
     return d;
 }
@@ -416,17 +466,45 @@ namespace tc {
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Diagonal class of rows [r0, r1) (see kDiagGeneral / kDiagNone): the
+// multiply adds the dense-diagonal terms of such a tile without searching the
+// shapes per row, with the same terms in the same order as diag_row.
+static int diag_class(const tc_plan *p, int r0, int r1)
+{
+    if (p->dia_shapes == 0 || r1 <= p->row_start || r0 >= p->row_stop) return kDiagNone;
+    int found = -1;
+    for (int s = 0; s < p->dia_shapes; ++s) {
+        if (r1 <= p->h_xStart[s] || r0 >= p->h_xStop[s]) continue;
+        if (found >= 0) return kDiagGeneral;        // two shapes share rows of the tile
+        found = s;
+    }
+    if (found < 0) return kDiagNone;
+    const int xs = p->h_xStart[found], xe = p->h_xStop[found], msub = xe - xs;
+    if (r0 < xs || r1 > xe || r0 < p->row_start || r1 > p->row_stop) return kDiagGeneral;
+    for (int n = p->h_nDiasPtr[found]; n < p->h_nDiasPtr[found + 1]; ++n) {
+        const int off = p->h_offsets[n];
+        if (r0 - xs + off < 0 || r1 - 1 - xs + off >= msub) return kDiagGeneral;
+    }
+    return found + 1 < kDiagNone ? found + 1 : kDiagGeneral;
+}
+
 tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStream_t stream)
 {
     const int M = p->M;
     std::vector<Tile> tiles;
-    plan_tiles(csrRow, M, p->params, tiles, &p->ntiles_vector, &p->ntiles_long);
+    plan_tiles(csrRow, M, p->params, 4 * num_sms(), tiles, &p->ntiles_vector, &p->ntiles_long);
+    p->ntiles_lanes = 0;
+    for (const Tile &t : tiles) {
+        p->ntiles_lanes += tile_kind(t) <= TILE_L32 || tile_kind(t) == TILE_MERGE;
+        if (tile_nrows(t) < 1 || tile_nrows(t) > kMaxTileNrows)
+            return fail(TC_ERR_FORMAT, "tile of %d rows", tile_nrows(t));
+    }
     p->ntiles = (int)tiles.size();
     p->nnz_csr = csrRow[M];
     // shared-memory stage sizes (ints, multiples of 4) from the largest tile
     int max_rows = 1, max_nnz = 0;
     for (const Tile &t : tiles)
-        if (tile_kind(t) != TILE_LONG) {
+        if (tile_kind(t) != TILE_LONG && tile_kind(t) < TILE_STREAM) {
             max_rows = std::max(max_rows, tile_nrows(t));
             max_nnz = std::max(max_nnz, t.nnz);
         }
@@ -447,6 +525,7 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
                 return fail(TC_ERR_FORMAT, "offsets of shape %d are not increasing", s);
         p->max_span = std::max(p->max_span, p->h_offsets[sd[s].y - 1] - p->h_offsets[sd[s].x]);
     }
+    for (Tile &t : tiles) t.nrows_kind |= diag_class(p, t.row0, t.row0 + tile_nrows(t)) << 12;
 
     size_t o_rp = 0;
     size_t o_cols = align256(o_rp + sizeof(int) * ((size_t)M + 1) + 16);

@@ -233,13 +233,31 @@ __device__ __forceinline__ float diag_row(const DevPlan &p, const float *__restr
     return acc;
 }
 
+// Shared memory of the merge and stream tiles: one union per kernel, used by
+// every instantiation of the tile code in that kernel.
+struct MergeSmem {
+    float rsum[kMergeRows];
+    float carry[kBlock];
+    int crow[kBlock];
+};
+union TileSmem {
+    MergeSmem merge;
+    float4 vals4[kStreamNnz / 4 + 2];   // stream tiles: the tile's aligned word window
+    float vals[kStreamNnz + 8];
+};
+__device__ __forceinline__ TileSmem &tile_smem()
+{
+    __shared__ TileSmem s;
+    return s;
+}
+
 template <bool SIGNED, class Src>
 __device__ void tile_merge(const DevPlan &p, const Tile &t, const Src &src,
                            const float *__restrict__ x, float *__restrict__ y, bool wait)
 {
-    __shared__ float rsum[kMergeRows];
-    __shared__ float carry[kBlock];
-    __shared__ int crow[kBlock];
+    float *const rsum = tile_smem().merge.rsum;
+    float *const carry = tile_smem().merge.carry;
+    int *const crow = tile_smem().merge.crow;
     const int nr = tile_nrows(t), nz = t.nnz, row0 = t.row0, tid = threadIdx.x;
     const int total = nr + nz;
     const int L = (total + kBlock - 1) / kBlock;
@@ -296,6 +314,174 @@ __device__ void tile_merge(const DevPlan &p, const Tile &t, const Src &src,
     __syncthreads();                              // rsum / carry are reused by the next tile
 }
 
+// ---------------------------------------------------------------- stream tile
+// Entry-parallel gather, row-parallel sum.  The tile's CSR words are read as
+// the 16-byte aligned int4s that cover them, coalesced across the CTA (the
+// cols array is 256-byte aligned and zero-padded past its end, so the window
+// never leaves it); each thread turns its kStreamQ int4s per round into
+// kStreamQ * 4 signed x terms, all loads in flight together, and stores them
+// as float4s in shared memory at their window position (entry j of the tile
+// at vals[lead + j]).  Words of the window outside the tile are valid column
+// words of neighbouring tiles (or the zero padding, column 0), so their
+// gathers stay inside x and their slots are never read.  Then each row's
+// dense-diagonal terms (offset order) and entries (stored order) are added
+// by one thread: the order of tile_rows_seq, so a matrix gets the same y from
+// every one-lane tile kind.  TILE_STREAM strides single rows over the CTA;
+// TILE_STREAM4 gives each thread runs of 4 consecutive rows (int4
+// row-pointer loads, float4 y stores) for tiles of many short rows.  The
+// first round's CSR words and the row pointers are immutable plan data, read
+// before wait_prior_grid().
+constexpr int kStreamQ = 2;   // int4 CSR words per thread per round
+
+struct StreamWords {
+    const int4 *cq;   // aligned-down start of the tile's CSR words
+    int lead;         // words before nz0 in the first int4
+    int nq;           // int4s covering the tile
+    int4 w[kStreamQ]; // this thread's first-round words
+};
+
+__device__ __forceinline__ void stream_words_first(const DevPlan &p, const Tile &t, StreamWords &sw)
+{
+    sw.lead = t.nz0 & 3;
+    sw.cq = reinterpret_cast<const int4 *>(p.cols + (t.nz0 - sw.lead));
+    sw.nq = (sw.lead + t.nnz + 3) >> 2;
+#pragma unroll
+    for (int q = 0; q < kStreamQ; ++q) {
+        const int i = threadIdx.x + q * kBlock;
+        sw.w[q] = i < sw.nq ? __ldg(sw.cq + i) : make_int4(0, 0, 0, 0);
+    }
+}
+
+// vals[lead + j] = signed x term of entry j of the tile; ends with a barrier.
+template <bool SIGNED>
+__device__ __forceinline__ void stream_gather(const float *__restrict__ x, float *vals, StreamWords &sw)
+{
+    const int tid = threadIdx.x;
+    for (int base = 0; base < sw.nq; base += kStreamQ * kBlock) {
+        if (base > 0) {
+#pragma unroll
+            for (int q = 0; q < kStreamQ; ++q) {
+                const int i = base + tid + q * kBlock;
+                sw.w[q] = i < sw.nq ? __ldg(sw.cq + i) : make_int4(0, 0, 0, 0);
+            }
+        }
+        float4 v[kStreamQ];
+#pragma unroll
+        for (int q = 0; q < kStreamQ; ++q) {
+            if (base + tid + q * kBlock < sw.nq) {
+                v[q].x = gather<SIGNED>(x, sw.w[q].x);
+                v[q].y = gather<SIGNED>(x, sw.w[q].y);
+                v[q].z = gather<SIGNED>(x, sw.w[q].z);
+                v[q].w = gather<SIGNED>(x, sw.w[q].w);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kStreamQ; ++q) {
+            const int i = base + tid + q * kBlock;
+            if (i < sw.nq) reinterpret_cast<float4 *>(vals)[i] = v[q];
+        }
+    }
+    __syncthreads();
+}
+
+// Dense-diagonal terms of row r of a tile of diagonal class dc: the terms
+// and order of diag_row, without the per-row shape search when the class
+// names the tile's one shape.
+__device__ __forceinline__ float diag_tile_row(const DevPlan &p, const float *__restrict__ x, int dc, int r)
+{
+    if (dc == kDiagNone) return 0.f;
+    if (dc == kDiagGeneral) return diag_row(p, x, r);
+    const int4 sh = __ldg(p.shapes + dc - 1);
+    const int2 dr = __ldg(p.shape_dias + dc - 1);
+    const float *__restrict__ xr = x + (r - sh.x + sh.z);
+    float acc = 0.f;
+    for (int d = dr.x; d < dr.y; ++d) acc += __ldg(xr + __ldg(p.offsets + d));
+    return acc;
+}
+
+template <bool SIGNED>
+__device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                            float *__restrict__ y, bool wait)
+{
+    float *const vals = tile_smem().vals;
+    constexpr int RQ = kStreamRows / kBlock;
+    const int tid = threadIdx.x, nr = tile_nrows(t), row0 = t.row0, dc = tile_dclass(t);
+    StreamWords sw;
+    stream_words_first(p, t, sw);
+    const int base = t.nz0 - sw.lead;                           // rowptr value of vals[0]
+    int rb[RQ], re[RQ];
+#pragma unroll
+    for (int k = 0; k < RQ; ++k) {
+        const int rl = tid + k * kBlock;
+        const bool ok = rl < nr;
+        rb[k] = ok ? __ldg(p.rowptr + row0 + rl) - base : 0;
+        re[k] = ok ? __ldg(p.rowptr + row0 + rl + 1) - base : 0;
+    }
+    if (wait) wait_prior_grid();
+    stream_gather<SIGNED>(x, vals, sw);
+#pragma unroll
+    for (int k = 0; k < RQ; ++k) {
+        const int rl = tid + k * kBlock;
+        if (rl < nr) {
+            float acc = diag_tile_row(p, x, dc, row0 + rl);
+            for (int j = rb[k]; j < re[k]; ++j) acc += vals[j];
+            y[row0 + rl] = acc;
+        }
+    }
+    __syncthreads();                                            // vals is reused by the next tile
+}
+
+// TILE_STREAM4: row0 is a multiple of 4 (the row pointers' int4 loads are
+// aligned; the array is padded by 16 bytes past rowptr[M], and rows past the
+// tile are masked), at most kStream4Rows rows.
+template <bool SIGNED>
+__device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                             float *__restrict__ y, bool wait)
+{
+    float *const vals = tile_smem().vals;
+    constexpr int GQ = kStream4Rows / (4 * kBlock);             // row groups per thread
+    const int tid = threadIdx.x, nr = tile_nrows(t), row0 = t.row0, dc = tile_dclass(t);
+    StreamWords sw;
+    stream_words_first(p, t, sw);
+    const int base = t.nz0 - sw.lead;
+    int4 rp[GQ];
+    int rp4[GQ];
+#pragma unroll
+    for (int k = 0; k < GQ; ++k) {
+        const int g = 4 * (tid + k * kBlock);                   // first row of the group
+        const bool ok = g < nr;
+        rp[k] = ok ? __ldg(reinterpret_cast<const int4 *>(p.rowptr + row0 + g)) : make_int4(0, 0, 0, 0);
+        rp4[k] = ok ? __ldg(p.rowptr + row0 + min(g + 4, nr)) : 0;
+    }
+    if (wait) wait_prior_grid();
+    stream_gather<SIGNED>(x, vals, sw);
+#pragma unroll
+    for (int k = 0; k < GQ; ++k) {
+        const int g = 4 * (tid + k * kBlock);
+        if (g >= nr) continue;
+        const int b[5] = {rp[k].x - base, rp[k].y - base, rp[k].z - base, rp[k].w - base, rp4[k] - base};
+        float acc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            acc[u] = 0.f;
+            if (g + u < nr) {
+                acc[u] = diag_tile_row(p, x, dc, row0 + g + u);
+                const int e = g + u + 1 < nr ? b[u + 1] : b[4];
+                for (int j = b[u]; j < e; ++j) acc[u] += vals[j];
+            }
+        }
+        float *yr = y + row0 + g;
+        if (g + 4 <= nr && (reinterpret_cast<uintptr_t>(yr) & 15) == 0) {
+            *reinterpret_cast<float4 *>(yr) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (g + u < nr) yr[u] = acc[u];
+        }
+    }
+    __syncthreads();                                            // vals is reused by the next tile
+}
+
 // One row with more entries than the planner's per-tile limit: the whole CTA
 // strides over it; warp sums are combined in warp order.
 template <bool SIGNED>
@@ -350,6 +536,8 @@ __device__ __forceinline__ void run_tile_src(const DevPlan &p, const Tile &t, co
 {
     switch (tile_kind(t)) {
     case TILE_MERGE: tile_merge<SIGNED>(p, t, src, x, y, wait); break;
+    case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, wait); break;
+    case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, wait); break;
     case TILE_L1: tile_rows_seq<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_L2: tile_rows<SIGNED, 2>(p, t, src, x, y, wait); break;
     case TILE_L4: tile_rows<SIGNED, 4>(p, t, src, x, y, wait); break;

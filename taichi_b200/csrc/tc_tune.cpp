@@ -147,9 +147,9 @@ extern "C" tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const
         f.neg_offsets = best_plan->h_offsets.data();
         f.csrRow = rp.data(); f.csrCol = cw.data();
         // {tile_mode, tile_rows, max_lanes, ctas_per_sm}, most promising first
-        const int cand[][4] = {{0, 512, 32, 4}, {0, 2048, 32, 4}, {0, 256, 32, 4}, {0, 1024, 32, 2},
-                               {0, 1024, 32, 8}, {0, 512, 32, 8}, {0, 2048, 32, 2}, {1, 1024, 32, 4},
-                               {1, 1024, 8, 4}, {0, 256, 32, 8}, {1, 1024, 32, 2}, {0, 512, 32, 2}};
+        const int cand[][4] = {{2, 1024, 32, 4}, {2, 2048, 32, 4}, {1, 1024, 32, 4}, {0, 512, 32, 4},
+                               {2, 512, 32, 4}, {0, 2048, 32, 4}, {1, 1024, 8, 4}, {0, 1024, 32, 8},
+                               {1, 1024, 32, 2}, {0, 256, 32, 4}, {0, 512, 32, 8}, {0, 1024, 32, 2}};
         for (const auto &cnd : cand) {
                     if (st != TC_OK || trials >= max_trials) break;
                     tc_params q = best.params;

@@ -30,7 +30,7 @@ def solo(plan, x, M, dev):
     return y.cpu().numpy()
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3], ids=["batched", "plain", "batched_dev", "plain_dev"])
 def test_served_results_identical_to_solo(tc, dev, mode):
     import torch
     plans, mats = make_plans(tc)
@@ -45,14 +45,21 @@ def test_served_results_identical_to_solo(tc, dev, mode):
     for r in range(n):
         M, N, rp, col = mats[matrix[r]]
         x = torch.from_numpy(rng.uniform(-1, 1, N).astype(np.float32)).pin_memory()
-        xs.append(x)
-        ys.append(torch.full((M,), float("nan")).pin_memory())
         want.append(solo(plans[matrix[r]], x.numpy(), M, dev))
+        if mode & tc.SERVE_DEVICE_VECTORS:
+            xs.append(x.to(dev))
+            ys.append(torch.full((M,), float("nan"), device=dev))
+        else:
+            xs.append(x)
+            ys.append(torch.full((M,), float("nan")).pin_memory())
     stats, lat = srv.run(arrival, [ids[m] for m in matrix], xs, ys, mode=mode)
+    torch.cuda.synchronize()
+    xs = [x.cpu() for x in xs]
+    ys = [y.cpu() for y in ys]
     for r in range(n):
         np.testing.assert_array_equal(ys[r].numpy(), want[r], err_msg="request %d" % r)
     assert stats["requests"] == n and (lat > 0).all()
-    if mode == 0:
+    if mode & 1 == 0:
         assert stats["mean_batch"] > 1.0          # requests were batched together
     print("mode %d: %.0f SpMV/s, p50 %.3f ms, p99 %.3f ms, mean batch %.1f" % (
         mode, stats["spmv_per_s"], stats["p50_ms"], stats["p99_ms"], stats["mean_batch"]))

@@ -110,6 +110,58 @@ def test_tile_kinds_and_edges(tc, dev, tile):
     check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "edges%s" % (tile,))
 
 
+MODE_CASES = [c for c in PARTITION_CASES if c["name"] in
+              ("band_holes", "multi_shape", "many_shapes", "rmat16_selfloops", "overlap")]
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["merge", "lanes", "stream"])
+@pytest.mark.parametrize("case", MODE_CASES, ids=[c["name"] for c in MODE_CASES])
+def test_tile_modes(tc, dev, case, mode):
+    """Every tile mode against the oracle, hybrid and plain plans."""
+    M, N, rp, col = cases.matrix(case)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(tile_mode=mode))
+    check_plan(plan, fmt, M, N, rp, col, dev, "%s/mode%d" % (case["name"], mode))
+    plan.close()
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(tile_mode=mode), partition=False)
+    check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "%s/plain/mode%d" % (case["name"], mode))
+    plan.close()
+
+
+@pytest.mark.parametrize("tile", [(1024, 4096), (1, 1), (3, 7), (2040, 8192), (64, 100), (1024, 2048)])
+def test_stream_tiles_edges(tc, dev, tile):
+    """Stream tiles next to lane and long tiles, unaligned tile starts, empty
+    rows, and the tile caps at their extremes."""
+    rng = np.random.default_rng(12)
+    lengths = np.concatenate([np.zeros(301, int), rng.integers(0, 3, 2003), [5000, 0, 9000],
+                              rng.integers(30, 200, 50), [1], np.zeros(5, int), [127, 128, 129],
+                              rng.integers(0, 12, 3001), [70000], rng.integers(0, 2, 5000)])
+    M, N = len(lengths), 7001
+    rp, col = csr_from_lengths(lengths, N, 5)
+    prm = tc.params(tile_rows=tile[0], tile_nnz=tile[1], tile_mode=2)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=prm, partition=False)
+    check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "stream%s" % (tile,))
+    plan.close()
+
+
+def test_stream_matches_sequential_rows(tc, dev):
+    """Stream tiles add a row's terms in the order of one-lane tiles, so the
+    two give bit-identical FP32 y when every row is short."""
+    import torch
+    for name in ("band_holes", "rmat16_selfloops"):
+        case = next(c for c in cases.MATRIX_CASES if c["name"] == name)
+        M, N, rp, col = cases.matrix(case)
+        assert np.diff(rp).max() <= 128
+        fmt, _ = oracle.partition(M, N, rp, col)
+        x = np.random.default_rng(9).uniform(-1, 1, N).astype(np.float32)
+        ys = []
+        for mode in (1, 2):
+            plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(tile_mode=mode, max_lanes=1))
+            ys.append(run_spmv(plan, x, M, dev))
+            plan.close()
+        np.testing.assert_array_equal(ys[0], ys[1], err_msg=name)
+
+
 def test_empty_and_tiny(tc, dev):
     import torch
     # no non-zeros at all
