@@ -12,7 +12,10 @@ FP32 x uniform in [-1, 1].
 resident in HBM; the timed region replays a CUDA graph of back-to-back SpMVs
 that rotate over enough resident copies of the matrix and vectors (> 2x the
 126 MB L2) that every SpMV reads its operands from HBM.  `e2e` is the same
-metric through tc_spmv_host (pinned host x in, host y out, synchronous).
+metric through the host-vector API: every step copies its x in from pinned
+host memory and its y out; steps alternate two staging slots on two streams
+(tc_spmv_host_async), so one step's copy-in overlaps the previous step's
+copy-out; `e2e.sync_value` is the synchronous tc_spmv_host, one step at a time.
 With --impl reference the reference's CPU SpMV loop (main.cu:61-69, restated
 in the oracle) runs on all host cores on the same matrix.
 
@@ -167,8 +170,12 @@ def run_ours(args, rank, world, local_rank):
         over["tile_rows"] = args.tile_rows
     if args.rows_strided:
         over["flags"] = tc.TC_FLAG_ROWS_STRIDED
+    if args.no_direct:
+        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_DIRECT
     if args.tile_nnz is not None:
         over["tile_nnz"] = args.tile_nnz
+    if args.ctas_per_sm is not None:
+        over["ctas_per_sm"] = args.ctas_per_sm
     prm = tc.params(**over)
     try:
         plan0 = tc.Plan.from_csr(M, N, rp, col, prm=prm, stream=stream)
@@ -265,23 +272,41 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     warm_ms = ev0.elapsed_time(ev1) / 256
 
-    # end to end through the public host API (pinned host buffers)
-    hx = torch.from_numpy(x_host).pin_memory()
-    hy = torch.empty(M, dtype=torch.float32).pin_memory()
-    e2e_steps = max(3, min(args.steps, 200))
+    # end to end through the public host API (pinned host buffers): every step
+    # copies its x in and its y out.  Headline: tc_spmv_host_async with two
+    # staging slots on two streams, so one step's x copy-in overlaps the
+    # previous step's y copy-out; also the synchronous tc_spmv_host.
+    hxs = [torch.from_numpy(x_host).pin_memory() for _ in range(2)]
+    hys = [torch.empty(M, dtype=torch.float32).pin_memory() for _ in range(2)]
+    e2e_steps = max(3, min(args.steps, 400))
     for _ in range(3):
-        plan0.spmv_host(hx, hy, stream=stream)
+        plan0.spmv_host(hxs[0], hys[0], stream=stream)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        plan0.spmv_host(hx, hy, stream=stream)
+        plan0.spmv_host(hxs[0], hys[0], stream=stream)
+    sync_s = (time.perf_counter() - t0) / e2e_steps
+    streams = [stream, torch.cuda.Stream(dev)]
+    for i in range(4):
+        plan0.spmv_host_async(hxs[i & 1], hys[i & 1], i & 1, streams[i & 1])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        plan0.spmv_host_async(hxs[i & 1], hys[i & 1], i & 1, streams[i & 1])
+    for s in streams:
+        s.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
+    plan0.check()
+    assert np.array_equal(hys[0].numpy(), hys[1].numpy()), "pipelined host multiply mismatch"
     e2e_gbs = bytes_per / e2e_s / 1e9 * world
+    e2e_sync_gbs = bytes_per / sync_s / 1e9 * world
 
+    # DRAM bytes per launch of the multiply from one ncu capture of this
+    # workload with the default parameters (profiles/traffic.json)
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and not over:
         with open(tf) as f:
-            traffic = json.load(f).get("spmv_tiles_kernel/" + args.workload)
+            traffic = json.load(f).get(args.workload)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -310,7 +335,9 @@ def run_ours(args, rank, world, local_rank):
                          "unit": "GB/s", "frac": round(gbs / world / peak, 4),
                          "peak_kind": peak_kind + " hbm_gbs (copy)", "traffic": traffic},
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 4 * N,
-                    "d2h_bytes_per_step": 4 * M, "ms_per_step": e2e_s * 1e3},
+                    "d2h_bytes_per_step": 4 * M, "ms_per_step": e2e_s * 1e3,
+                    "api": "tc_spmv_host_async, 2 slots on 2 streams",
+                    "sync_value": round(e2e_sync_gbs, 3), "sync_api": "tc_spmv_host"},
             "gpu_launches": args.steps,
             "clocks": cl,
             "cpu_baseline": cpu,
@@ -525,6 +552,8 @@ def main():
     ap.add_argument("--tile-rows", type=int, default=None, help="most rows per multiply tile")
     ap.add_argument("--rows-strided", action="store_true", help="stream tiles: one row per thread")
     ap.add_argument("--tile-nnz", type=int, default=None, help="entry limit of a tile")
+    ap.add_argument("--ctas-per-sm", type=int, default=None, help="resident CTAs per SM (persistent grids)")
+    ap.add_argument("--no-direct", action="store_true", help="stream tiles only, no direct tiles")
     args = ap.parse_args()
     if args.impl == "ours" and args.form != "plain":
         {"spmm": run_spmm, "batched": run_batched, "served": run_served}[args.form](args)

@@ -58,7 +58,7 @@ typedef struct tc_params {
                              threads (merge path); 1: lanes per row chosen
                              from the tile's row lengths; 2: stream tiles
                              (entry-parallel gather into shared memory, then
-                             row sums), one CTA per tile (1)                   */
+                             row sums), one CTA per tile (2)                   */
     int flags;            /* TC_FLAG_*                                         */
 } tc_params;
 
@@ -69,6 +69,9 @@ typedef struct tc_params {
                                      when the previous kernel has finished)  */
 #define TC_FLAG_ROWS_STRIDED 0x8  /* stream tiles (tile_mode 2) sum one row
                                      per thread, never 4 consecutive rows   */
+#define TC_FLAG_NO_DIRECT    0x10 /* tile_mode 2: no direct tiles (4-row runs
+                                     read straight from global memory) for
+                                     rows averaging at most one entry       */
 
 TC_API void tc_params_default(tc_params *p);
 
@@ -144,6 +147,16 @@ TC_API tc_status tc_spmv(const tc_plan *plan, const float *d_x, float *d_y, void
 /* Same multiply on host buffers: copies x in, multiplies, copies y out and
  * waits.  Pinned host buffers give the full link bandwidth. */
 TC_API tc_status tc_spmv_host(const tc_plan *plan, const float *h_x, float *h_y, void *stream);
+
+/* The same three steps enqueued on `stream` without waiting, through the
+ * plan's staging slot `slot` (0 or 1; slot 0 is the one tc_spmv_host uses).
+ * h_y holds y once the stream has reached this point.  Calls on one slot must
+ * be ordered on the device (same stream, or an event between streams); two
+ * slots on two streams let one call's x copy-in overlap another's y copy-out.
+ * No counterpart in the reference (its taichi_SpMV copies synchronously,
+ * TaiChi.cu:1357-1420). */
+TC_API tc_status tc_spmv_host_async(const tc_plan *plan, const float *h_x, float *h_y, int slot,
+                                    void *stream);
 
 /* Y = A X for k right-hand sides (1 <= k <= 64).  X is N x k row-major with
  * leading dimension ldx >= k, Y is M x k with ldy >= k; device memory. */

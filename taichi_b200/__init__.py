@@ -20,6 +20,7 @@ TC_FLAG_NO_PARTITION = 0x1
 TC_FLAG_KEEP_HOST = 0x2
 TC_FLAG_NO_PDL = 0x4
 TC_FLAG_ROWS_STRIDED = 0x8
+TC_FLAG_NO_DIRECT = 0x10
 
 _IP = C.POINTER(C.c_int)
 
@@ -57,7 +58,8 @@ class PlanInfo(C.Structure):
 EXPORTS = (
     "tc_params_default", "tc_last_error", "tc_status_string", "tc_plan_create",
     "tc_plan_from_format", "tc_plan_destroy", "tc_plan_info_get", "tc_plan_export",
-    "tc_plan_thumbnail", "tc_plan_check", "tc_spmv", "tc_spmv_host", "tc_spmm", "tc_getsdf",
+    "tc_plan_thumbnail", "tc_plan_check", "tc_spmv", "tc_spmv_host", "tc_spmv_host_async",
+    "tc_spmm", "tc_getsdf",
     "tc_trace_contours", "tc_read_mtx", "tc_free", "tc_batch_create", "tc_batch_run",
     "tc_batch_graph_launch", "tc_batch_destroy", "tc_tune", "tc_tune_cache_clear",
     "tc_serve_config_default", "tc_server_create", "tc_server_admit", "tc_server_evict",
@@ -94,6 +96,7 @@ def lib():
         L.tc_plan_check.argtypes = [vp]
         L.tc_spmv.argtypes = [vp, vp, vp, vp]
         L.tc_spmv_host.argtypes = [vp, vp, vp, vp]
+        L.tc_spmv_host_async.argtypes = [vp, vp, vp, C.c_int, vp]
         L.tc_spmm.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp]
         L.tc_getsdf.argtypes = [C.c_int, C.c_int, vp, vp, C.POINTER(Params), _IP, _IP, vp,
                                 C.c_int, _IP, vp, vp]
@@ -400,6 +403,11 @@ class Plan:
 
     def spmv_host(self, x, y, stream=None):
         check(lib().tc_spmv_host(self._h, _ptr(x), _ptr(y), _stream(stream)))
+
+    def spmv_host_async(self, x, y, slot, stream):
+        """Enqueue copy-in, multiply, copy-out through staging slot 0 or 1;
+        y is ready once `stream` has reached this point."""
+        check(lib().tc_spmv_host_async(self._h, _ptr(x), _ptr(y), slot, _stream(stream)))
 
     def spmm(self, X, Y, k=None, ldx=None, ldy=None, stream=None):
         if k is None:

@@ -67,7 +67,7 @@ void tc_params_default(tc_params *p)
     p->tile_nnz = 2048;
     p->max_lanes = 32;
     p->ctas_per_sm = 4;
-    p->tile_mode = 1;
+    p->tile_mode = 2;
     p->flags = 0;
 }
 
@@ -168,6 +168,8 @@ tc_status tc_plan_destroy(tc_plan *p)
     if (p->dev) cudaFree(p->dev);
     if (p->d_xbuf) cudaFree(p->d_xbuf);
     if (p->d_ybuf) cudaFree(p->d_ybuf);
+    if (p->d_xbuf1) cudaFree(p->d_xbuf1);
+    if (p->d_ybuf1) cudaFree(p->d_ybuf1);
     delete p;
     return TC_OK;
 }
@@ -229,21 +231,39 @@ tc_status tc_spmv(const tc_plan *p, const float *d_x, float *d_y, void *stream)
     return tc::launch_spmv(p->dev_plan(), d_x, d_y, (cudaStream_t)stream);
 }
 
+// Copy x in, multiply, copy y out on `stream`, through the plan's staging
+// slot `slot` (device x / y buffers allocated on first use).
+static tc_status spmv_host_enqueue(tc_plan *p, const float *h_x, float *h_y, int slot, cudaStream_t s)
+{
+    float *&dx = slot ? p->d_xbuf1 : p->d_xbuf;
+    float *&dy = slot ? p->d_ybuf1 : p->d_ybuf;
+    if (!dx) {
+        cudaError_t e1 = cudaMalloc(&dx, sizeof(float) * ((size_t)p->N + 4));
+        cudaError_t e2 = cudaMalloc(&dy, sizeof(float) * ((size_t)p->M + 4));
+        if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(TC_ERR_ALLOC, "x/y staging buffers");
+    }
+    if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x, sizeof(float) * (size_t)p->N, cudaMemcpyHostToDevice, s));
+    TC_CHECK(tc::launch_spmv(p->dev_plan(), dx, dy, s));
+    if (p->M) TC_CUDA(cudaMemcpyAsync(h_y, dy, sizeof(float) * (size_t)p->M, cudaMemcpyDeviceToHost, s));
+    return TC_OK;
+}
+
 tc_status tc_spmv_host(const tc_plan *cp, const float *h_x, float *h_y, void *stream)
 {
     tc_plan *p = const_cast<tc_plan *>(cp);
     if (!p || (!h_x && p->N) || (!h_y && p->M)) return fail(TC_ERR_INVALID, "tc_spmv_host: null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    if (!p->d_xbuf) {
-        cudaError_t e1 = cudaMalloc(&p->d_xbuf, sizeof(float) * ((size_t)p->N + 4));
-        cudaError_t e2 = cudaMalloc(&p->d_ybuf, sizeof(float) * ((size_t)p->M + 4));
-        if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(TC_ERR_ALLOC, "x/y staging buffers");
-    }
-    if (p->N) TC_CUDA(cudaMemcpyAsync(p->d_xbuf, h_x, sizeof(float) * (size_t)p->N, cudaMemcpyHostToDevice, s));
-    TC_CHECK(tc::launch_spmv(p->dev_plan(), p->d_xbuf, p->d_ybuf, s));
-    if (p->M) TC_CUDA(cudaMemcpyAsync(h_y, p->d_ybuf, sizeof(float) * (size_t)p->M, cudaMemcpyDeviceToHost, s));
+    TC_CHECK(spmv_host_enqueue(p, h_x, h_y, 0, s));
     TC_CUDA(cudaStreamSynchronize(s));
     return tc_plan_check(p);
+}
+
+tc_status tc_spmv_host_async(const tc_plan *cp, const float *h_x, float *h_y, int slot, void *stream)
+{
+    tc_plan *p = const_cast<tc_plan *>(cp);
+    if (!p || (!h_x && p->N) || (!h_y && p->M) || slot < 0 || slot > 1)
+        return fail(TC_ERR_INVALID, "tc_spmv_host_async: null argument or slot not 0/1");
+    return spmv_host_enqueue(p, h_x, h_y, slot, (cudaStream_t)stream);
 }
 
 tc_status tc_spmm(const tc_plan *p, const float *d_X, int ldx, int k, float *d_Y, int ldy, void *stream)
@@ -364,7 +384,10 @@ namespace tc {
 
 tc_status ensure_smem(const void *kernel, size_t bytes)
 {
-    if (bytes <= 48 * 1024) return TC_OK;
+    // The default limit covers 48 KB of static + dynamic shared memory, so a
+    // kernel with static shared memory may need the attribute for less than
+    // 48 KB of dynamic memory too: set it for every size not yet granted.
+    if (bytes == 0) return TC_OK;
     int dev = 0;
     TC_CUDA(cudaGetDevice(&dev));
     static std::mutex mu;

@@ -1,11 +1,18 @@
-// tc_batch.cu -- many resident plans multiplied in one persistent launch.
+// tc_batch.cu -- many resident plans multiplied in one launch.
 //
 // The batch flattens the tile lists of all its plans into one work list of
-// (plan, tile) pairs in plan order and launches one grid of
-// (SMs x resident CTAs) CTAs that stride over it.  Every tile runs the same
-// device code as the single-plan kernel, so each matrix's y is bit-identical
-// alone and inside a batch.  The launch can be captured once in a CUDA graph
-// and replayed (tc_batch_graph_launch).
+// (plan, tile) pairs -- the plain plans' tiles first, then the hybrid plans'
+// -- and runs it with one CTA per work item: one launch for the plain part and
+// one for the hybrid part, so each runs tile code of one word kind only.  The
+// item's plan descriptor is read once into shared memory.  A CTA per item
+// keeps the most independent tiles in flight per SM; a
+// persistent grid that walks items in turn serialises each tile's load ->
+// gather -> sum chain per CTA and measured slower.  When every plan holds
+// only stream, direct and long tiles the lean kernels (no lane-tile code,
+// more CTAs per SM) run.  Every tile runs the same device code as the
+// single-plan kernel, so each matrix's y is bit-identical alone and inside a
+// batch.  The launches are captured once in a CUDA graph and replayed
+// (tc_batch_graph_launch).
 
 #include <cuda_runtime.h>
 
@@ -24,20 +31,22 @@ struct BatchItem {
     int tile;
 };
 
-__global__ void __launch_bounds__(kBlock) batch_kernel(const DevPlan *__restrict__ plans,
-                                                       const BatchItem *__restrict__ items,
-                                                       int nitems, const float *const *xs,
-                                                       float *const *ys)
+// Work items of plain plans (SIGNED = false) or of hybrid plans (true): the
+// work list holds the plain plans' items first, and each half runs under
+// its own kernel so that neither tile code raises the other's registers.
+template <bool SIGNED, bool LEAN>
+__global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned : kLeanMinBlocks) : 1)
+    batch_kernel(const DevPlan *__restrict__ plans, const BatchItem *__restrict__ items, int nitems,
+                 const float *const *xs, float *const *ys)
 {
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
-        const BatchItem it = items[w];
-        const DevPlan &p = plans[it.plan];     // read in place (global memory)
-        const Tile t = p.tiles[it.tile];
-        const float *x = xs[it.plan];
-        float *y = ys[it.plan];
-        if (p.hybrid) run_tile<true>(p, t, x, y);
-        else run_tile<false>(p, t, x, y);
-    }
+    __shared__ DevPlan sp;                     // the item's plan, read by every thread
+    if ((int)blockIdx.x >= nitems) return;     // the grid has one CTA per item
+    const BatchItem it = items[blockIdx.x];
+    if (threadIdx.x == 0) sp = plans[it.plan];
+    __syncthreads();
+    const Tile t = sp.tiles[it.tile];
+    if (LEAN) run_lean_tile<SIGNED>(sp, t, xs[it.plan], ys[it.plan], true);
+    else run_tile<SIGNED>(sp, t, xs[it.plan], ys[it.plan]);
 }
 
 }  // namespace
@@ -46,7 +55,9 @@ __global__ void __launch_bounds__(kBlock) batch_kernel(const DevPlan *__restrict
 struct tc_batch {
     int n = 0;
     int nitems = 0;
+    int nplain = 0;      // items of plain plans (the first ones of the list)
     int grid = 0;
+    bool lean = false;
     size_t smem = 0;
     void *dev = nullptr;
     tc::DevPlan *d_plans = nullptr;
@@ -68,15 +79,23 @@ tc_status tc_batch_create(int n, tc_plan *const *plans, const float *const *d_x,
     *out = nullptr;
     std::vector<tc::DevPlan> dps(n);
     std::vector<tc::BatchItem> items;
+    bool lean = true;
     for (int i = 0; i < n; ++i) {
         if (!plans[i]) return fail(TC_ERR_INVALID, "plan %d is null", i);
         dps[i] = plans[i]->dev_plan();
-        for (int t = 0; t < dps[i].ntiles; ++t) items.push_back(tc::BatchItem{i, t});
+        lean = lean && dps[i].per_tile == 2;
     }
+    for (int pass = 0; pass < 2; ++pass)     // plain plans' items, then hybrid plans'
+        for (int i = 0; i < n; ++i)
+            if (dps[i].hybrid == pass)
+                for (int t = 0; t < dps[i].ntiles; ++t) items.push_back(tc::BatchItem{i, t});
     tc_batch *b = new (std::nothrow) tc_batch();
     if (!b) return fail(TC_ERR_ALLOC, "host allocation");
+    b->lean = lean;
     b->n = n;
     b->nitems = (int)items.size();
+    b->nplain = 0;
+    for (const tc::BatchItem &it : items) b->nplain += dps[it.plan].hybrid == 0;
     b->smem = 0;
     size_t o_pl = 0;
     size_t o_it = (sizeof(tc::DevPlan) * n + 255) & ~(size_t)255;
@@ -95,17 +114,12 @@ tc_status tc_batch_create(int n, tc_plan *const *plans, const float *const *d_x,
         e = cudaMemcpy(b->d_items, items.data(), sizeof(tc::BatchItem) * items.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_x, d_x, sizeof(void *) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_y, d_y, sizeof(void *) * n, cudaMemcpyHostToDevice);
-    int per_sm = 0, dev = 0, sms = 0;
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::batch_kernel, tc::kBlock, b->smem);
-    if (e == cudaSuccess) e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) {
         cudaFree(base);
         delete b;
         return fail(TC_ERR_CUDA, "tc_batch_create: %s", cudaGetErrorString(e));
     }
-    b->grid = std::max(1, std::min(b->nitems, std::max(1, per_sm) * sms));
+    b->grid = std::max(1, b->nitems);                   // one CTA per work item
     *out = b;
     return TC_OK;
 }
@@ -114,8 +128,16 @@ tc_status tc_batch_run(tc_batch *b, void *stream)
 {
     if (!b) return fail(TC_ERR_INVALID, "null batch");
     if (b->nitems == 0) return TC_OK;
-    tc::batch_kernel<<<b->grid, tc::kBlock, b->smem, (cudaStream_t)stream>>>(
-        b->d_plans, b->d_items, b->nitems, b->d_x, b->d_y);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int np = b->nplain, nh = b->nitems - b->nplain;   // one CTA per item
+    const tc::BatchItem *hi = b->d_items + np;
+    if (b->lean) {
+        if (np) tc::batch_kernel<false, true><<<np, tc::kBlock, 0, s>>>(b->d_plans, b->d_items, np, b->d_x, b->d_y);
+        if (nh) tc::batch_kernel<true, true><<<nh, tc::kBlock, 0, s>>>(b->d_plans, hi, nh, b->d_x, b->d_y);
+    } else {
+        if (np) tc::batch_kernel<false, false><<<np, tc::kBlock, 0, s>>>(b->d_plans, b->d_items, np, b->d_x, b->d_y);
+        if (nh) tc::batch_kernel<true, false><<<nh, tc::kBlock, 0, s>>>(b->d_plans, hi, nh, b->d_x, b->d_y);
+    }
     TC_CUDA(cudaGetLastError());
     return TC_OK;
 }

@@ -49,7 +49,8 @@ enum TileKind : int {
     TILE_LONG = 6,
     TILE_MERGE = 7,    // merge-path split of rows and entries over the CTA's threads
     TILE_STREAM = 8,   // entry-parallel gather, then row-parallel sums in shared memory
-    TILE_STREAM4 = 9   // the same with 4 consecutive rows per thread (row0 % 4 == 0)
+    TILE_STREAM4 = 9,  // the same with 4 consecutive rows per thread (row0 % 4 == 0)
+    TILE_DIRECT4 = 10  // 4 consecutive rows per thread straight from global memory
 };
 
 struct Tile {          // 16 bytes, read once per CTA
@@ -75,9 +76,10 @@ constexpr int kBlock = 256;           // threads per CTA of the multiply kernels
 constexpr int kMaxTileRows = 1 << 20; // planner limit on rows per tile
 constexpr int kStageNnz = 8192;       // CSR words of a tile staged in shared memory
 constexpr int kStreamNnz = 4096;      // most entries of a TILE_STREAM tile
-constexpr int kStreamRows = 1024;     // most rows of a TILE_STREAM tile (4 per thread)
+constexpr int kStreamRows = 256;      // most rows of a TILE_STREAM tile (1 per thread)
 constexpr int kStreamRowMax = 128;    // longer rows leave stream tiles for lane tiles
 constexpr int kStream4Rows = 1024;    // most rows of a TILE_STREAM4 tile (a run of 4 per thread)
+constexpr int kDirectRows = 1024;     // most rows of a direct tile (TILE_DIRECT4)
 
 // Everything a multiply kernel needs about one plan (passed by value).
 struct DevPlan {
@@ -131,7 +133,8 @@ struct tc_plan {
     std::vector<unsigned char> thumb_stages;   // 5*H*W when kept
     std::vector<int> corners;                   // 4 per kept contour
     // device staging for tc_spmv_host
-    float *d_xbuf = nullptr, *d_ybuf = nullptr;
+    float *d_xbuf = nullptr, *d_ybuf = nullptr;     // slot 0
+    float *d_xbuf1 = nullptr, *d_ybuf1 = nullptr;   // slot 1 (tc_spmv_host_async)
 
     tc::DevPlan dev_plan() const;
     int64_t spmv_bytes() const;

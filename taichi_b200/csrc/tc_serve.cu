@@ -39,27 +39,33 @@ struct ReqDesc {
 
 constexpr int kMaxBatch = 256;
 
-// One launch over the tiles of up to kMaxBatch requests.
-__global__ void __launch_bounds__(kBlock) serve_kernel(const DevPlan *__restrict__ plans,
-                                                       const ReqDesc *__restrict__ reqs, int nreq,
-                                                       int total_tiles)
+// One CTA per tile of nreq requests whose matrices all have plain (SIGNED =
+// false) or all hybrid words; request i owns tiles [reqs[i].tile_begin,
+// reqs[i + 1].tile_begin) of the grid.  Thread 0 finds the CTA's request by
+// binary search and parks its plan descriptor in shared memory.  LEAN: every
+// admitted plan holds only stream, direct and long tiles.
+template <bool SIGNED, bool LEAN>
+__global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned : kLeanMinBlocks) : 1)
+    serve_kernel(const DevPlan *__restrict__ plans, const ReqDesc *__restrict__ reqs, int nreq)
 {
-    __shared__ int begin[kMaxBatch + 1];
-    for (int i = threadIdx.x; i < nreq; i += blockDim.x) begin[i] = reqs[i].tile_begin;
-    if (threadIdx.x == 0) begin[nreq] = total_tiles;
-    __syncthreads();
-    for (int g = blockIdx.x; g < total_tiles; g += gridDim.x) {
-        int lo = 0, hi = nreq;                     // begin[lo] <= g < begin[hi]
+    __shared__ DevPlan sp;
+    __shared__ ReqDesc sr;
+    __shared__ int stile;
+    const int g = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nreq;                     // tile_begin[lo] <= g < tile_begin[hi]
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (begin[mid] <= g) lo = mid; else hi = mid;
+            if (reqs[mid].tile_begin <= g) lo = mid; else hi = mid;
         }
-        const ReqDesc rq = reqs[lo];
-        const DevPlan &p = plans[rq.plan];
-        const Tile t = p.tiles[g - rq.tile_begin];
-        if (p.hybrid) run_tile<true>(p, t, rq.x, rq.y, false);
-        else run_tile<false>(p, t, rq.x, rq.y, false);
+        sr = reqs[lo];
+        sp = plans[sr.plan];
+        stile = g - sr.tile_begin;
     }
+    __syncthreads();
+    const Tile t = sp.tiles[stile];
+    if (LEAN) run_lean_tile<SIGNED>(sp, t, sr.x, sr.y, false);
+    else run_tile<SIGNED>(sp, t, sr.x, sr.y, false);
 }
 
 double now_s()
@@ -90,7 +96,12 @@ struct tc_server {
     tc::DevPlan *d_plans = nullptr;
     int max_plans = 0;
     int sms = 148;
+    int nonlean = 0;                       // admitted plans with lane or merge tiles
 };
+
+namespace {
+bool lean_plan(const tc_plan *p) { return p->dev_plan().per_tile == 2; }
+}  // namespace
 
 namespace {
 
@@ -174,6 +185,7 @@ tc_status tc_server_admit(tc_server *sv, tc_plan *plan, int *id)
     TC_CUDA(cudaMemcpy(sv->d_plans + slot, &dp, sizeof dp, cudaMemcpyHostToDevice));
     sv->plans[slot] = plan;
     sv->footprint[slot] = fp;
+    sv->nonlean += lean_plan(plan) ? 0 : 1;
     sv->used += fp;
     *id = slot;
     return TC_OK;
@@ -184,6 +196,7 @@ tc_status tc_server_evict(tc_server *sv, int id)
     if (!sv || id < 0 || id >= (int)sv->plans.size() || !sv->plans[id])
         return fail(TC_ERR_INVALID, "tc_server_evict: no such matrix");
     sv->used -= sv->footprint[id];
+    sv->nonlean -= lean_plan(sv->plans[id]) ? 0 : 1;
     sv->plans[id] = nullptr;
     sv->footprint[id] = 0;
     return TC_OK;
@@ -226,6 +239,8 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
         }
     } else {           // continuous batching over the launch contexts
         std::deque<int> pending;
+        std::vector<tc::ReqDesc> batch;    // the batch being packed, arrival order
+        std::vector<int> order;            // its request indices
         int next = 0, completed = 0;
         while (completed < nreq) {
             const double now = tc::now_s() - t0;
@@ -249,32 +264,52 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
             tc_server::Ctx &c = *free_ctx;
             // pack arrived requests into the arena
             int64_t used = 0;
-            int tiles = 0;
             int nb = 0;
+            batch.clear();
+            order.clear();
             while (!pending.empty() && nb < sv->cfg.max_batch) {
                 const int r = pending.front();
                 const tc_plan *p = sv->plans[matrix[r]];
                 if (device_vectors) {   // the request's own device x and y
-                    c.h_desc[nb] = tc::ReqDesc{matrix[r], tiles, h_x[r], h_y[r]};
+                    batch.push_back(tc::ReqDesc{matrix[r], 0, h_x[r], h_y[r]});
                 } else {                // x and y slots in the context's arena
                     const int64_t need = slot_floats(p->N) + slot_floats(p->M);
                     if ((used + need) * 4 > sv->cfg.arena_bytes) break;
                     float *dx = c.arena + used, *dy = dx + slot_floats(p->N);
                     used += need;
-                    c.h_desc[nb] = tc::ReqDesc{matrix[r], tiles, dx, dy};
+                    batch.push_back(tc::ReqDesc{matrix[r], 0, dx, dy});
                     if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x[r], 4 * (size_t)p->N, cudaMemcpyHostToDevice, c.s));
                 }
-                tiles += p->ntiles;
-                c.reqs.push_back(r);
+                order.push_back(r);
                 pending.pop_front();
                 ++nb;
             }
+            // plain matrices' requests first, then hybrid ones: one launch each,
+            // one CTA per tile, tiles numbered from 0 within each launch
+            int np = 0, tiles[2] = {0, 0};
+            for (int pass = 0, k = 0; pass < 2; ++pass)
+                for (int i = 0; i < nb; ++i) {
+                    const tc_plan *p = sv->plans[batch[i].plan];
+                    if (p->hybrid != pass) continue;
+                    c.h_desc[k] = batch[i];
+                    c.h_desc[k].tile_begin = tiles[pass];
+                    tiles[pass] += p->ntiles;
+                    c.reqs.push_back(order[i]);
+                    np += pass == 0;
+                    ++k;
+                }
             TC_CUDA(cudaMemcpyAsync(c.d_desc, c.h_desc, sizeof(tc::ReqDesc) * nb, cudaMemcpyHostToDevice, c.s));
-            if (tiles > 0) {
-                const int grid = std::max(1, std::min(tiles, sv->sms * 8));
-                tc::serve_kernel<<<grid, tc::kBlock, 0, c.s>>>(sv->d_plans, c.d_desc, nb, tiles);
-                TC_CUDA(cudaGetLastError());
+            const bool lean = sv->nonlean == 0;
+            if (tiles[0] > 0) {
+                if (lean) tc::serve_kernel<false, true><<<tiles[0], tc::kBlock, 0, c.s>>>(sv->d_plans, c.d_desc, np);
+                else tc::serve_kernel<false, false><<<tiles[0], tc::kBlock, 0, c.s>>>(sv->d_plans, c.d_desc, np);
             }
+            if (tiles[1] > 0) {
+                const tc::ReqDesc *hd = c.d_desc + np;
+                if (lean) tc::serve_kernel<true, true><<<tiles[1], tc::kBlock, 0, c.s>>>(sv->d_plans, hd, nb - np);
+                else tc::serve_kernel<true, false><<<tiles[1], tc::kBlock, 0, c.s>>>(sv->d_plans, hd, nb - np);
+            }
+            TC_CUDA(cudaGetLastError());
             for (int i = 0; i < nb && !device_vectors; ++i) {
                 const int r = c.reqs[i];
                 const tc_plan *p = sv->plans[matrix[r]];

@@ -59,25 +59,31 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, int min_tiles, std::
             continue;
         }
         if (prm.tile_mode == 2 && rp[r + 1] - rp[r] <= kStreamRowMax) {
-            // stream tile: short rows up to the row and entry caps; a tile
+            // stream tile: short rows up to the row and entry caps.  A run
             // that starts on a multiple of 4 rows and holds many rows runs 4
-            // consecutive rows per thread (TILE_STREAM4)
+            // consecutive rows per thread: read directly from global memory
+            // when they average at most one entry (TILE_DIRECT4), through
+            // shared memory when at most two (TILE_STREAM4); otherwise one
+            // row per thread (TILE_STREAM)
             const bool a4 = (r & 3) == 0 && !(prm.flags & TC_FLAG_ROWS_STRIDED);
-            const int cap_rows = std::min(rows_cap, a4 ? kStream4Rows : kStreamRows);
+            const int cap_rows = std::min(rows_cap, a4 ? kDirectRows : kStreamRows);
             const int cap_nnz = std::max(1, std::min(2 * prm.tile_nnz, spread));
             int n = 0;
             while (r + n < M && n < cap_rows && rp[r + n + 1] - rp[r + n] <= kStreamRowMax &&
                    rp[r + n + 1] - rp[r] <= cap_nnz)
                 ++n;
             if (n == 0) n = 1;        // a single row longer than cap_nnz but <= kStreamRowMax
-            const bool four = a4 && n >= 2 * kBlock;
-            if (!four) n = std::min(n, kStreamRows);
+            const int ent = rp[r + n] - rp[r];
+            const bool direct = a4 && n >= 2 * kBlock && ent <= n && !(prm.flags & TC_FLAG_NO_DIRECT);
+            const bool four = !direct && a4 && n >= 2 * kBlock && ent <= 2 * n;
+            if (!direct) n = std::min(n, four ? kStream4Rows : kStreamRows);
             if (r + n < M) {          // end on a multiple of 256 rows (whole row sweeps), else of 4
                 const int cut = (r + n) & ~255;
                 if (cut - r >= 256) n = cut - r;
                 else if (n > 4) n -= (r + n) & 3;
             }
-            tiles.push_back(Tile{r, rp[r], rp[r + n] - rp[r], tile_word(n, four ? TILE_STREAM4 : TILE_STREAM)});
+            const int kind = direct ? TILE_DIRECT4 : four ? TILE_STREAM4 : TILE_STREAM;
+            tiles.push_back(Tile{r, rp[r], rp[r + n] - rp[r], tile_word(n, kind)});
             r += n;
             continue;
         }
@@ -249,11 +255,7 @@ __global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned 
     allow_next_grid();
     const Tile t = p.tiles[blockIdx.x];
     if (LEAN) {
-        switch (tile_kind(t)) {
-        case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, true); break;
-        case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, true); break;
-        default: long_row<SIGNED>(p, t, x, y, true); break;
-        }
+        run_lean_tile<SIGNED>(p, t, x, y, true);
     } else {
         run_tile<SIGNED>(p, t, x, y, true);
     }

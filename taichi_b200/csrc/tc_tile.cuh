@@ -215,7 +215,10 @@ __device__ __forceinline__ int merge_split(const Src &src, int nr, int nz, int d
     return lo;
 }
 
-// Dense-diagonal terms of one row, offsets in order.
+// Dense-diagonal terms of one row, offsets in order, kDiagU offsets' loads
+// issued before their adds (a wide band's terms do not wait on each other).
+constexpr int kDiagU = 4;
+
 __device__ __forceinline__ float diag_row(const DevPlan &p, const float *__restrict__ x, int r)
 {
     float acc = 0.f;
@@ -225,9 +228,18 @@ __device__ __forceinline__ float diag_row(const DevPlan &p, const float *__restr
         if (r < sh.x || r >= sh.y) continue;
         const int2 dr = __ldg(p.shape_dias + s);
         const int cb = r - sh.x + sh.z;
-        for (int d = dr.x; d < dr.y; ++d) {
-            const int c = cb + __ldg(p.offsets + d);
-            if (c >= sh.z && c < sh.z + sh.w) acc += __ldg(x + c);
+        for (int d = dr.x; d < dr.y; d += kDiagU) {
+            float v[kDiagU];
+            bool in[kDiagU];
+#pragma unroll
+            for (int k = 0; k < kDiagU; ++k) {
+                const int c = d + k < dr.y ? cb + __ldg(p.offsets + d + k) : -1;
+                in[k] = c >= sh.z && c < sh.z + sh.w;
+                v[k] = in[k] ? __ldg(x + c) : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kDiagU; ++k)
+                if (in[k]) acc += v[k];
         }
     }
     return acc;
@@ -395,7 +407,14 @@ __device__ __forceinline__ float diag_tile_row(const DevPlan &p, const float *__
     const int2 dr = __ldg(p.shape_dias + dc - 1);
     const float *__restrict__ xr = x + (r - sh.x + sh.z);
     float acc = 0.f;
-    for (int d = dr.x; d < dr.y; ++d) acc += __ldg(xr + __ldg(p.offsets + d));
+    for (int d = dr.x; d < dr.y; d += kDiagU) {
+        float v[kDiagU];
+#pragma unroll
+        for (int k = 0; k < kDiagU; ++k) v[k] = d + k < dr.y ? __ldg(xr + __ldg(p.offsets + d + k)) : 0.f;
+#pragma unroll
+        for (int k = 0; k < kDiagU; ++k)
+            if (d + k < dr.y) acc += v[k];
+    }
     return acc;
 }
 
@@ -482,6 +501,85 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
     __syncthreads();                                            // vals is reused by the next tile
 }
 
+// Direct tiles: runs of 4 consecutive rows per thread, read straight from
+// global memory with no shared memory and no barrier -- for tiles whose rows
+// average at most one entry, where a thread's 4 rows hold a handful of
+// consecutive CSR words.  Row pointers come as one int4 (row0 % 4 == 0) plus
+// the run's end; the first kDirectW words of the run and their gathers are
+// all in flight together, each word added to the row that owns it (words in
+// stored order, after the row's dense-diagonal terms: the order of
+// tile_rows_seq); a run with more words walks the rest one at a time.  A
+// thread owns G runs (rows 4 * (tid + k * kBlock) + u), all their loads in
+// flight together; TILE_DIRECT4 (G = 1) holds up to 1024 rows.  (G = 2,
+// 2048-row tiles, measured slower on R-MAT: half the CTAs, twice the chain.)
+constexpr int kDirectW = 4;
+
+template <bool SIGNED, int G>
+__device__ void tile_direct(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                            float *__restrict__ y, bool wait)
+{
+    const int nr = tile_nrows(t), row0 = t.row0, dc = tile_dclass(t);
+    int b[G][5];
+    int c[G][kDirectW];
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+        const int g = 4 * (threadIdx.x + k * kBlock);           // first row of group k
+        if (g < nr) {
+            const int4 r4 = __ldg(reinterpret_cast<const int4 *>(p.rowptr + row0 + g));
+            const int e4 = __ldg(p.rowptr + row0 + min(g + 4, nr));
+            // row u of the group holds words [b[u], b[u+1]); rows past the tile hold none
+            b[k][0] = r4.x;
+            b[k][1] = g + 1 < nr ? r4.y : e4;
+            b[k][2] = g + 2 < nr ? r4.z : e4;
+            b[k][3] = g + 3 < nr ? r4.w : e4;
+            b[k][4] = e4;
+        } else {
+            b[k][0] = b[k][1] = b[k][2] = b[k][3] = b[k][4] = 0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < G; ++k)
+#pragma unroll
+        for (int w = 0; w < kDirectW; ++w)
+            c[k][w] = b[k][0] + w < b[k][4] ? __ldg(p.cols + b[k][0] + w) : 0;
+    if (wait) wait_prior_grid();
+    float v[G][kDirectW];
+#pragma unroll
+    for (int k = 0; k < G; ++k)
+#pragma unroll
+        for (int w = 0; w < kDirectW; ++w)
+            v[k][w] = b[k][0] + w < b[k][4] ? gather<SIGNED>(x, c[k][w]) : 0.f;
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+        const int g = 4 * (threadIdx.x + k * kBlock);
+        if (g >= nr) continue;
+        float acc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] = g + u < nr ? diag_tile_row(p, x, dc, row0 + g + u) : 0.f;
+#pragma unroll
+        for (int w = 0; w < kDirectW; ++w) {
+            const int j = b[k][0] + w;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j >= b[k][u] && j < b[k][u + 1]) acc[u] += v[k][w];
+        }
+        for (int j = b[k][0] + kDirectW; j < b[k][4]; ++j) {   // groups with more words
+            const float z = gather<SIGNED>(x, __ldg(p.cols + j));
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j >= b[k][u] && j < b[k][u + 1]) acc[u] += z;
+        }
+        float *yr = y + row0 + g;
+        if (g + 4 <= nr && (reinterpret_cast<uintptr_t>(yr) & 15) == 0) {
+            *reinterpret_cast<float4 *>(yr) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (g + u < nr) yr[u] = acc[u];
+        }
+    }
+}
+
 // One row with more entries than the planner's per-tile limit: the whole CTA
 // strides over it; warp sums are combined in warp order.
 template <bool SIGNED>
@@ -538,12 +636,27 @@ __device__ __forceinline__ void run_tile_src(const DevPlan &p, const Tile &t, co
     case TILE_MERGE: tile_merge<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, wait); break;
     case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, wait); break;
+    case TILE_DIRECT4: tile_direct<SIGNED, 1>(p, t, x, y, wait); break;
     case TILE_L1: tile_rows_seq<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_L2: tile_rows<SIGNED, 2>(p, t, src, x, y, wait); break;
     case TILE_L4: tile_rows<SIGNED, 4>(p, t, src, x, y, wait); break;
     case TILE_L8: tile_rows<SIGNED, 8>(p, t, src, x, y, wait); break;
     case TILE_L16: tile_rows<SIGNED, 16>(p, t, src, x, y, wait); break;
     case TILE_L32: tile_rows<SIGNED, 32>(p, t, src, x, y, wait); break;
+    default: long_row<SIGNED>(p, t, x, y, wait); break;
+    }
+}
+
+// The tile kinds of a stream plan (tile_mode 2 without lane tiles): kernels
+// that only ever see these carry no lane-tile code and fit more CTAs per SM.
+template <bool SIGNED>
+__device__ __forceinline__ void run_lean_tile(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                                              float *__restrict__ y, bool wait)
+{
+    switch (tile_kind(t)) {
+    case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, wait); break;
+    case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, wait); break;
+    case TILE_DIRECT4: tile_direct<SIGNED, 1>(p, t, x, y, wait); break;
     default: long_row<SIGNED>(p, t, x, y, wait); break;
     }
 }

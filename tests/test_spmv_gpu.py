@@ -145,9 +145,8 @@ def test_stream_tiles_edges(tc, dev, tile):
 
 
 def test_stream_matches_sequential_rows(tc, dev):
-    """Stream tiles add a row's terms in the order of one-lane tiles, so the
-    two give bit-identical FP32 y when every row is short."""
-    import torch
+    """Stream and direct tiles add a row's terms in the order of one-lane
+    tiles, so all give bit-identical FP32 y when every row is short."""
     for name in ("band_holes", "rmat16_selfloops"):
         case = next(c for c in cases.MATRIX_CASES if c["name"] == name)
         M, N, rp, col = cases.matrix(case)
@@ -155,11 +154,28 @@ def test_stream_matches_sequential_rows(tc, dev):
         fmt, _ = oracle.partition(M, N, rp, col)
         x = np.random.default_rng(9).uniform(-1, 1, N).astype(np.float32)
         ys = []
-        for mode in (1, 2):
-            plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(tile_mode=mode, max_lanes=1))
+        for mode, flags in ((1, 0), (2, 0), (2, tc.TC_FLAG_NO_DIRECT), (2, tc.TC_FLAG_ROWS_STRIDED)):
+            plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(tile_mode=mode, max_lanes=1, flags=flags))
             ys.append(run_spmv(plan, x, M, dev))
             plan.close()
-        np.testing.assert_array_equal(ys[0], ys[1], err_msg=name)
+        for k in range(1, len(ys)):
+            np.testing.assert_array_equal(ys[0], ys[k], err_msg="%s variant %d" % (name, k))
+
+
+def test_direct_tiles(tc, dev):
+    """Direct tiles (rows averaging at most one entry) next to stream, lane
+    and long tiles, with an unaligned tail, against the oracle, with and
+    without direct tiles."""
+    rng = np.random.default_rng(21)
+    lengths = np.concatenate([rng.integers(0, 2, 5003), rng.integers(0, 12, 2000), [300, 0, 7],
+                              rng.integers(0, 3, 4097), rng.integers(5, 9, 900), rng.integers(0, 2, 2051)])
+    M, N = len(lengths), 9000
+    rp, col = csr_from_lengths(lengths, N, 8)
+    for rows, flags in ((1024, 0), (2048, 0), (1024, tc.TC_FLAG_NO_DIRECT)):
+        prm = tc.params(tile_mode=2, tile_rows=rows, flags=flags)
+        plan = tc.Plan.from_csr(M, N, rp, col, prm=prm, partition=False)
+        check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "direct/rows%d/flags%d" % (rows, flags))
+        plan.close()
 
 
 def test_empty_and_tiny(tc, dev):
@@ -204,6 +220,29 @@ def test_spmv_host_e2e(tc, dev):
     y = np.zeros(M, np.float32)
     plan.spmv_host(x, y)
     np.testing.assert_array_equal(y.astype(np.float64), oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64)))
+
+
+def test_spmv_host_async_two_slots(tc, dev):
+    """Pipelined host multiplies: six requests alternate two staging slots on
+    two streams; each y equals the oracle's (integer x: exact)."""
+    import torch
+    M, N, rp, col = cases.matrix(cases.MATRIX_CASES[1])
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    rng = np.random.default_rng(5)
+    xs = [torch.from_numpy(rng.integers(-8, 9, N).astype(np.float32)).pin_memory() for _ in range(6)]
+    ys = [torch.full((M,), float("nan")).pin_memory() for _ in range(6)]
+    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    for i in range(6):
+        plan.spmv_host_async(xs[i], ys[i], i & 1, streams[i & 1])
+    for s in streams:
+        s.synchronize()
+    plan.check()
+    for i in range(6):
+        want = oracle.spmv_csr_f64(M, rp, col, xs[i].numpy().astype(np.float64))
+        np.testing.assert_array_equal(ys[i].numpy().astype(np.float64), want, err_msg="request %d" % i)
+    with pytest.raises(tc.TcError):
+        plan.spmv_host_async(xs[0], ys[0], 2, streams[0])
+    plan.close()
 
 
 def test_format_rejected(tc):
