@@ -72,6 +72,9 @@ typedef struct tc_params {
 #define TC_FLAG_NO_DIRECT    0x10 /* tile_mode 2: no direct tiles (4-row runs
                                      read straight from global memory) for
                                      rows averaging at most one entry       */
+#define TC_FLAG_NO_WIDE      0x20 /* tile_mode 2: no wide direct tiles (a
+                                     1024-thread CTA per 4096 rows) for a
+                                     matrix whose rows all qualify          */
 
 TC_API void tc_params_default(tc_params *p);
 

@@ -21,6 +21,7 @@ TC_FLAG_KEEP_HOST = 0x2
 TC_FLAG_NO_PDL = 0x4
 TC_FLAG_ROWS_STRIDED = 0x8
 TC_FLAG_NO_DIRECT = 0x10
+TC_FLAG_NO_WIDE = 0x20
 
 _IP = C.POINTER(C.c_int)
 

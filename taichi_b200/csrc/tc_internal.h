@@ -50,25 +50,27 @@ enum TileKind : int {
     TILE_MERGE = 7,    // merge-path split of rows and entries over the CTA's threads
     TILE_STREAM = 8,   // entry-parallel gather, then row-parallel sums in shared memory
     TILE_STREAM4 = 9,  // the same with 4 consecutive rows per thread (row0 % 4 == 0)
-    TILE_DIRECT4 = 10  // 4 consecutive rows per thread straight from global memory
+    TILE_DIRECT4 = 10,    // 4 consecutive rows per thread straight from global memory
+    TILE_DIRECT_WIDE = 11 // the same over up to 4096 rows (a 1024-thread CTA)
 };
 
 struct Tile {          // 16 bytes, read once per CTA
     int row0;          // first row
     int nz0;           // first CSR entry (rowptr[row0])
     int nnz;           // CSR entries of the tile
-    int nrows_kind;    // nrows (bits 0-11) | diagonal class << 12 (16 bits) | kind << 28
+    int nrows_kind;    // nrows (bits 0-12) | diagonal class << 13 (15 bits) | kind << 28
 };
 
 // Diagonal class of a tile: how its rows meet the dense-diagonal shapes.
 constexpr int kDiagGeneral = 0;        // per-row search over the shapes
-constexpr int kDiagNone = 0xffff;      // no row of the tile is in any shape
+constexpr int kDiagNone = 0x7fff;      // no row of the tile is in any shape
 // otherwise s + 1: every row lies in shape s alone and every offset of s
 // lands inside the shape's columns for every row of the tile
-constexpr int kMaxTileNrows = 0xfff;
+constexpr int kMaxTileNrows = 0x1fff;
+constexpr int kDiagShift = 13;
 
-__host__ __device__ inline int tile_nrows(const Tile &t) { return t.nrows_kind & 0xfff; }
-__host__ __device__ inline int tile_dclass(const Tile &t) { return (t.nrows_kind >> 12) & 0xffff; }
+__host__ __device__ inline int tile_nrows(const Tile &t) { return t.nrows_kind & 0x1fff; }
+__host__ __device__ inline int tile_dclass(const Tile &t) { return (t.nrows_kind >> kDiagShift) & 0x7fff; }
 __host__ __device__ inline int tile_kind(const Tile &t) { return (t.nrows_kind >> 28) & 0xf; }
 __host__ __device__ inline int tile_word(int nrows, int kind) { return nrows | (kind << 28); }
 
@@ -80,6 +82,8 @@ constexpr int kStreamRows = 256;      // most rows of a TILE_STREAM tile (1 per 
 constexpr int kStreamRowMax = 128;    // longer rows leave stream tiles for lane tiles
 constexpr int kStream4Rows = 1024;    // most rows of a TILE_STREAM4 tile (a run of 4 per thread)
 constexpr int kDirectRows = 1024;     // most rows of a direct tile (TILE_DIRECT4)
+constexpr int kDirectWideBlock = 1024; // threads of the direct kernel's CTAs
+constexpr int kDirectWideRows = 4 * kDirectWideBlock;   // most rows of a TILE_DIRECT_WIDE tile
 
 // Everything a multiply kernel needs about one plan (passed by value).
 struct DevPlan {
@@ -94,8 +98,9 @@ struct DevPlan {
     int pdl;                // launch with programmatic stream serialization
     int stage_rp, stage_cw; // ints per shared-memory stage (row pointers, CSR words)
     int grid;               // persistent grid size
-    int per_tile;           // one CTA per tile (stream plans): 1, or 2 when only stream
-                            // and long tiles occur (the lean kernel)
+    int per_tile;           // one CTA per tile (stream plans): 1, or 2 when only stream,
+                            // direct and long tiles occur (the lean kernel), or 3 when
+                            // every tile is a wide direct tile (the direct kernel)
     int *err;               // device error word (1: a bounded wait gave up)
 };
 
@@ -121,6 +126,7 @@ struct tc_plan {
     int2 *d_shape_dias = nullptr;
     int ntiles = 0, ntiles_vector = 0, ntiles_long = 0;
     int ntiles_lanes = 0;                // lane and merge tiles (TILE_L1..L32, TILE_MERGE)
+    int ntiles_wide = 0;                 // TILE_DIRECT_WIDE tiles (all or none)
     int max_span = 0;
     int stage_rp = 8, stage_cw = 8, grid = 1;
     int *d_err = nullptr;

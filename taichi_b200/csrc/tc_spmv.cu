@@ -50,6 +50,21 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, int min_tiles, std::
     const int rows_cap = std::max(1, std::min(prm.tile_rows, kMaxTileRows));
     tiles.clear();
     *nvec = *nlong = 0;
+    if (prm.tile_mode == 2 && prm.tile_rows >= kDirectRows &&
+        !(prm.flags & (TC_FLAG_NO_DIRECT | TC_FLAG_NO_WIDE | TC_FLAG_ROWS_STRIDED)) && M >= kDirectWideRows &&
+        rp[M] <= M) {
+        // rows of at most one entry on average and none long: the whole
+        // matrix as wide direct tiles (one 1024-thread CTA per 4096 rows)
+        bool short_rows = true;
+        for (int i = 0; i < M && short_rows; ++i) short_rows = rp[i + 1] - rp[i] <= kStreamRowMax;
+        if (short_rows) {
+            for (int r = 0; r < M; r += kDirectWideRows) {
+                const int n = std::min(kDirectWideRows, M - r);
+                tiles.push_back(Tile{r, rp[r], rp[r + n] - rp[r], tile_word(n, TILE_DIRECT_WIDE)});
+            }
+            return;
+        }
+    }
     int r = 0;
     while (r < M) {
         if (rp[r + 1] - rp[r] > long_len) {
@@ -244,6 +259,18 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
     if (!waited) wait_prior_grid();
 }
 
+// The multiply of a plan of wide direct tiles: one 1024-thread CTA per 4096
+// rows, one run of 4 rows per thread.  Few CTAs (the block scheduler's launch
+// cost grows with the CTA count) that all fit at once (2 per SM at 32
+// registers), each holding 1024 independent load chains.
+template <bool SIGNED>
+__global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan p, const float *__restrict__ x,
+                                                                     float *__restrict__ y)
+{
+    allow_next_grid();
+    direct_run<SIGNED>(p, p.tiles[blockIdx.x], x, y, true, 4 * threadIdx.x);
+}
+
 // The multiply of a stream plan: one CTA per tile, no shared-memory stages
 // (stream tiles read their CSR words as coalesced int4s; lane and long tiles
 // read global memory directly).  LEAN: the plan holds only stream and long
@@ -390,7 +417,7 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
     if (!dp.per_tile) TC_CHECK(ensure_smem((const void *)spmv_tiles_kernel<SIGNED>, smem));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(dp.per_tile ? dp.ntiles : dp.grid);
-    cfg.blockDim = dim3(kBlock);
+    cfg.blockDim = dim3(dp.per_tile == 3 ? kDirectWideBlock : kBlock);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -398,7 +425,8 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
     attr[0].val.programmaticStreamSerializationAllowed = dp.pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (dp.per_tile == 2) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, true>, dp, x, y));
+    if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED>, dp, x, y));
+    else if (dp.per_tile == 2) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, false>, dp, x, y));
     else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_tiles_kernel<SIGNED>, dp, x, y));
     return TC_OK;
@@ -451,7 +479,7 @@ tc::DevPlan tc_plan::dev_plan() const
     d.stage_rp = stage_rp;
     d.stage_cw = stage_cw;
     d.grid = grid;
-    d.per_tile = params.tile_mode != 2 ? 0 : (ntiles_lanes == 0 ? 2 : 1);
+    d.per_tile = params.tile_mode != 2 ? 0 : ntiles_wide == ntiles && ntiles > 0 ? 3 : ntiles_lanes == 0 ? 2 : 1;
     d.err = d_err;
     return d;
 }
@@ -496,6 +524,8 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     std::vector<Tile> tiles;
     plan_tiles(csrRow, M, p->params, 4 * num_sms(), tiles, &p->ntiles_vector, &p->ntiles_long);
     p->ntiles_lanes = 0;
+    p->ntiles_wide = 0;
+    for (const Tile &t : tiles) p->ntiles_wide += tile_kind(t) == TILE_DIRECT_WIDE;
     for (const Tile &t : tiles) {
         p->ntiles_lanes += tile_kind(t) <= TILE_L32 || tile_kind(t) == TILE_MERGE;
         if (tile_nrows(t) < 1 || tile_nrows(t) > kMaxTileNrows)
@@ -527,7 +557,7 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
                 return fail(TC_ERR_FORMAT, "offsets of shape %d are not increasing", s);
         p->max_span = std::max(p->max_span, p->h_offsets[sd[s].y - 1] - p->h_offsets[sd[s].x]);
     }
-    for (Tile &t : tiles) t.nrows_kind |= diag_class(p, t.row0, t.row0 + tile_nrows(t)) << 12;
+    for (Tile &t : tiles) t.nrows_kind |= diag_class(p, t.row0, t.row0 + tile_nrows(t)) << kDiagShift;
 
     size_t o_rp = 0;
     size_t o_cols = align256(o_rp + sizeof(int) * ((size_t)M + 1) + 16);

@@ -508,76 +508,70 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
 // the run's end; the first kDirectW words of the run and their gathers are
 // all in flight together, each word added to the row that owns it (words in
 // stored order, after the row's dense-diagonal terms: the order of
-// tile_rows_seq); a run with more words walks the rest one at a time.  A
-// thread owns G runs (rows 4 * (tid + k * kBlock) + u), all their loads in
-// flight together; TILE_DIRECT4 (G = 1) holds up to 1024 rows.  (G = 2,
-// 2048-row tiles, measured slower on R-MAT: half the CTAs, twice the chain.)
+// tile_rows_seq); a run with more words walks the rest one at a time.
+// TILE_DIRECT4 tiles (up to 1024 rows) give each of a 256-thread CTA's
+// threads one run; TILE_DIRECT_WIDE tiles (up to 4096 rows) are run by the
+// 1024-thread direct kernel, one run per thread, or by a 256-thread CTA as
+// four passes of runs (batch and served launches) -- the same rows, terms and
+// order either way.  (Two runs per thread with all loads in flight measured
+// slower on R-MAT; four run out of registers.)
 constexpr int kDirectW = 4;
 
-template <bool SIGNED, int G>
-__device__ void tile_direct(const DevPlan &p, const Tile &t, const float *__restrict__ x,
-                            float *__restrict__ y, bool wait)
+// The run of rows [g, g + 4) of tile t, g a multiple of 4.
+template <bool SIGNED>
+__device__ __forceinline__ void direct_run(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                                           float *__restrict__ y, bool wait, int g)
 {
     const int nr = tile_nrows(t), row0 = t.row0, dc = tile_dclass(t);
-    int b[G][5];
-    int c[G][kDirectW];
-#pragma unroll
-    for (int k = 0; k < G; ++k) {
-        const int g = 4 * (threadIdx.x + k * kBlock);           // first row of group k
-        if (g < nr) {
-            const int4 r4 = __ldg(reinterpret_cast<const int4 *>(p.rowptr + row0 + g));
-            const int e4 = __ldg(p.rowptr + row0 + min(g + 4, nr));
-            // row u of the group holds words [b[u], b[u+1]); rows past the tile hold none
-            b[k][0] = r4.x;
-            b[k][1] = g + 1 < nr ? r4.y : e4;
-            b[k][2] = g + 2 < nr ? r4.z : e4;
-            b[k][3] = g + 3 < nr ? r4.w : e4;
-            b[k][4] = e4;
-        } else {
-            b[k][0] = b[k][1] = b[k][2] = b[k][3] = b[k][4] = 0;
-        }
+    if (g >= nr) {
+        if (wait) wait_prior_grid();
+        return;
     }
+    const int4 r4 = __ldg(reinterpret_cast<const int4 *>(p.rowptr + row0 + g));
+    const int e4 = __ldg(p.rowptr + row0 + min(g + 4, nr));
+    // row u of the run holds words [b[u], b[u+1]); rows past the tile hold none
+    const int b[5] = {r4.x, g + 1 < nr ? r4.y : e4, g + 2 < nr ? r4.z : e4, g + 3 < nr ? r4.w : e4, e4};
+    int c[kDirectW];
 #pragma unroll
-    for (int k = 0; k < G; ++k)
-#pragma unroll
-        for (int w = 0; w < kDirectW; ++w)
-            c[k][w] = b[k][0] + w < b[k][4] ? __ldg(p.cols + b[k][0] + w) : 0;
+    for (int w = 0; w < kDirectW; ++w) c[w] = b[0] + w < e4 ? __ldg(p.cols + b[0] + w) : 0;
     if (wait) wait_prior_grid();
-    float v[G][kDirectW];
+    float v[kDirectW];
 #pragma unroll
-    for (int k = 0; k < G; ++k)
+    for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
+    float acc[4];
 #pragma unroll
-        for (int w = 0; w < kDirectW; ++w)
-            v[k][w] = b[k][0] + w < b[k][4] ? gather<SIGNED>(x, c[k][w]) : 0.f;
+    for (int u = 0; u < 4; ++u) acc[u] = g + u < nr ? diag_tile_row(p, x, dc, row0 + g + u) : 0.f;
 #pragma unroll
-    for (int k = 0; k < G; ++k) {
-        const int g = 4 * (threadIdx.x + k * kBlock);
-        if (g >= nr) continue;
-        float acc[4];
+    for (int w = 0; w < kDirectW; ++w) {
+        const int j = b[0] + w;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) acc[u] = g + u < nr ? diag_tile_row(p, x, dc, row0 + g + u) : 0.f;
-#pragma unroll
-        for (int w = 0; w < kDirectW; ++w) {
-            const int j = b[k][0] + w;
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (j >= b[k][u] && j < b[k][u + 1]) acc[u] += v[k][w];
-        }
-        for (int j = b[k][0] + kDirectW; j < b[k][4]; ++j) {   // groups with more words
-            const float z = gather<SIGNED>(x, __ldg(p.cols + j));
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (j >= b[k][u] && j < b[k][u + 1]) acc[u] += z;
-        }
-        float *yr = y + row0 + g;
-        if (g + 4 <= nr && (reinterpret_cast<uintptr_t>(yr) & 15) == 0) {
-            *reinterpret_cast<float4 *>(yr) = make_float4(acc[0], acc[1], acc[2], acc[3]);
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (g + u < nr) yr[u] = acc[u];
-        }
+        for (int u = 0; u < 4; ++u)
+            if (j >= b[u] && j < b[u + 1]) acc[u] += v[w];
     }
+    for (int j = b[0] + kDirectW; j < e4; ++j) {               // runs with more words
+        const float z = gather<SIGNED>(x, __ldg(p.cols + j));
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (j >= b[u] && j < b[u + 1]) acc[u] += z;
+    }
+    float *yr = y + row0 + g;
+    if (g + 4 <= nr && (reinterpret_cast<uintptr_t>(yr) & 15) == 0) {
+        *reinterpret_cast<float4 *>(yr) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (g + u < nr) yr[u] = acc[u];
+    }
+}
+
+// A direct tile in a 256-thread CTA: one pass (TILE_DIRECT4) or four
+// (TILE_DIRECT_WIDE).
+template <bool SIGNED>
+__device__ __forceinline__ void tile_direct(const DevPlan &p, const Tile &t, const float *__restrict__ x,
+                                            float *__restrict__ y, bool wait)
+{
+    const int passes = tile_kind(t) == TILE_DIRECT_WIDE ? kDirectWideRows / kDirectRows : 1;
+    for (int k = 0; k < passes; ++k) direct_run<SIGNED>(p, t, x, y, wait && k == 0, 4 * (threadIdx.x + k * kBlock));
 }
 
 // One row with more entries than the planner's per-tile limit: the whole CTA
@@ -636,7 +630,8 @@ __device__ __forceinline__ void run_tile_src(const DevPlan &p, const Tile &t, co
     case TILE_MERGE: tile_merge<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, wait); break;
     case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, wait); break;
-    case TILE_DIRECT4: tile_direct<SIGNED, 1>(p, t, x, y, wait); break;
+    case TILE_DIRECT4:
+    case TILE_DIRECT_WIDE: tile_direct<SIGNED>(p, t, x, y, wait); break;
     case TILE_L1: tile_rows_seq<SIGNED>(p, t, src, x, y, wait); break;
     case TILE_L2: tile_rows<SIGNED, 2>(p, t, src, x, y, wait); break;
     case TILE_L4: tile_rows<SIGNED, 4>(p, t, src, x, y, wait); break;
@@ -656,7 +651,8 @@ __device__ __forceinline__ void run_lean_tile(const DevPlan &p, const Tile &t, c
     switch (tile_kind(t)) {
     case TILE_STREAM4: tile_stream4<SIGNED>(p, t, x, y, wait); break;
     case TILE_STREAM: tile_stream<SIGNED>(p, t, x, y, wait); break;
-    case TILE_DIRECT4: tile_direct<SIGNED, 1>(p, t, x, y, wait); break;
+    case TILE_DIRECT4:
+    case TILE_DIRECT_WIDE: tile_direct<SIGNED>(p, t, x, y, wait); break;
     default: long_row<SIGNED>(p, t, x, y, wait); break;
     }
 }

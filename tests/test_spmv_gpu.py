@@ -154,12 +154,36 @@ def test_stream_matches_sequential_rows(tc, dev):
         fmt, _ = oracle.partition(M, N, rp, col)
         x = np.random.default_rng(9).uniform(-1, 1, N).astype(np.float32)
         ys = []
-        for mode, flags in ((1, 0), (2, 0), (2, tc.TC_FLAG_NO_DIRECT), (2, tc.TC_FLAG_ROWS_STRIDED)):
+        for mode, flags in ((1, 0), (2, 0), (2, tc.TC_FLAG_NO_WIDE), (2, tc.TC_FLAG_NO_DIRECT),
+                            (2, tc.TC_FLAG_ROWS_STRIDED)):
             plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(tile_mode=mode, max_lanes=1, flags=flags))
             ys.append(run_spmv(plan, x, M, dev))
             plan.close()
         for k in range(1, len(ys)):
             np.testing.assert_array_equal(ys[0], ys[k], err_msg="%s variant %d" % (name, k))
+
+
+@pytest.mark.parametrize("M", [4096, 10001, 3 * 4096 + 4])
+def test_wide_direct_tiles(tc, dev, M):
+    """A matrix whose rows all average at most one entry runs as wide direct
+    tiles (one 1024-thread CTA per 4096 rows): partial last tile and last run,
+    against the oracle; and the same y as 256-thread direct tiles."""
+    import torch
+    rng = np.random.default_rng(M)
+    lengths = rng.integers(0, 2, M)
+    lengths[rng.integers(0, M, 20)] = rng.integers(2, 60, 20)      # a few longer rows
+    N = M + 7
+    rp, col = csr_from_lengths(lengths, N, 9)
+    assert rp[-1] <= M
+    plan = tc.Plan.from_csr(M, N, rp, col, partition=False)
+    assert plan.info()["ntiles"] == (M + 4095) // 4096              # wide tiles
+    check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "wide/M%d" % M)
+    x = rng.uniform(-1, 1, N).astype(np.float32)
+    y_wide = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_WIDE), partition=False)
+    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_wide)
+    plan.close()
 
 
 def test_direct_tiles(tc, dev):
