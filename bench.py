@@ -489,7 +489,8 @@ def run_served(args):
     import taichi_b200 as tc
     dev = torch.device("cuda", 0)
     mats = pool_matrices("serve", 48, 11)
-    srv = tc.Server(contexts=3, max_batch=64, arena_bytes=512 << 20, hbm_budget=96 << 30)
+    srv = tc.Server(contexts=args.serve_contexts, max_batch=args.serve_max_batch, arena_bytes=512 << 20,
+                    hbm_budget=96 << 30)
     plans, ids = [], []
     for name, M, rp, col in mats:
         p = tc.Plan.from_csr(M, M, rp, col)
@@ -529,7 +530,8 @@ def run_served(args):
         summary[form] = {"batched_spmv_per_s_p99_lt_2ms": b, "plain_spmv_per_s_p99_lt_2ms": pl,
                          "ratio": round(b / pl, 2) if pl else None, "results": results}
     print(json.dumps({"form": "served", "requests": nreq, "pool": len(mats),
-                      "pool_rows": int(sum(m[1] for m in mats)), "summary": summary}), flush=True)
+                      "pool_rows": int(sum(m[1] for m in mats)), "contexts": args.serve_contexts,
+                      "max_batch": args.serve_max_batch, "summary": summary}), flush=True)
     srv.close()
 
 
@@ -543,9 +545,9 @@ def main():
     ap.add_argument("--form", default="plain", choices=["plain", "spmm", "batched", "served"])
     ap.add_argument("--tune-trials", type=int, default=8)
     ap.add_argument("--requests", type=int, default=20000)
-    ap.add_argument("--rates", type=float, nargs="+", default=[2000, 5000, 10000, 20000, 40000])
+    ap.add_argument("--rates", type=float, nargs="+", default=[2000, 5000, 10000, 15000, 20000, 40000])
     ap.add_argument("--device-rates", type=float, nargs="+",
-                    default=[10000, 20000, 50000, 100000, 200000, 400000])
+                    default=[20000, 40000, 50000, 60000, 100000, 125000, 150000, 175000, 200000])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tile-mode", type=int, default=None, help="0 merge, 1 lanes, 2 stream")
@@ -554,6 +556,8 @@ def main():
     ap.add_argument("--tile-nnz", type=int, default=None, help="entry limit of a tile")
     ap.add_argument("--ctas-per-sm", type=int, default=None, help="resident CTAs per SM (persistent grids)")
     ap.add_argument("--no-direct", action="store_true", help="stream tiles only, no direct tiles")
+    ap.add_argument("--serve-contexts", type=int, default=6, help="served form: launch contexts in flight")
+    ap.add_argument("--serve-max-batch", type=int, default=64, help="served form: most requests per launch")
     args = ap.parse_args()
     if args.impl == "ours" and args.form != "plain":
         {"spmm": run_spmm, "batched": run_batched, "served": run_served}[args.form](args)

@@ -269,7 +269,7 @@ typedef struct tc_server tc_server;
 typedef struct tc_serve_config {
     int64_t hbm_budget;   /* bytes for admitted plans + request arenas (64 GiB)    */
     int64_t arena_bytes;  /* device x / y space of one launch context (256 MiB)   */
-    int contexts;         /* launch contexts (streams) in flight (3)             */
+    int contexts;         /* launch contexts (streams) in flight (6)             */
     int max_batch;        /* most requests packed into one launch (64, <= 256)   */
     int max_plans;        /* size of the resident plan table (1024)              */
 } tc_serve_config;

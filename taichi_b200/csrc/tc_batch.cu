@@ -29,13 +29,14 @@ namespace {
 struct BatchItem {
     int plan;
     int tile;
+    int part;          // quarter of a wide direct tile, else 0
 };
 
 // Work items of plain plans (SIGNED = false) or of hybrid plans (true): the
 // work list holds the plain plans' items first, and each half runs under
 // its own kernel so that neither tile code raises the other's registers.
 template <bool SIGNED, bool LEAN>
-__global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned : kLeanMinBlocks) : 1)
+__global__ void __launch_bounds__(kBlock, LEAN ? kItemMinBlocks : 1)
     batch_kernel(const DevPlan *__restrict__ plans, const BatchItem *__restrict__ items, int nitems,
                  const float *const *xs, float *const *ys)
 {
@@ -45,8 +46,7 @@ __global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned 
     if (threadIdx.x == 0) sp = plans[it.plan];
     __syncthreads();
     const Tile t = sp.tiles[it.tile];
-    if (LEAN) run_lean_tile<SIGNED>(sp, t, xs[it.plan], ys[it.plan], true);
-    else run_tile<SIGNED>(sp, t, xs[it.plan], ys[it.plan]);
+    run_tile_part<SIGNED, LEAN>(sp, t, it.part, xs[it.plan], ys[it.plan], true);
 }
 
 }  // namespace
@@ -83,12 +83,14 @@ tc_status tc_batch_create(int n, tc_plan *const *plans, const float *const *d_x,
     for (int i = 0; i < n; ++i) {
         if (!plans[i]) return fail(TC_ERR_INVALID, "plan %d is null", i);
         dps[i] = plans[i]->dev_plan();
-        lean = lean && dps[i].per_tile == 2;
+        lean = lean && dps[i].per_tile >= 2;
     }
     for (int pass = 0; pass < 2; ++pass)     // plain plans' items, then hybrid plans'
         for (int i = 0; i < n; ++i)
             if (dps[i].hybrid == pass)
-                for (int t = 0; t < dps[i].ntiles; ++t) items.push_back(tc::BatchItem{i, t});
+                for (int t = 0; t < dps[i].ntiles; ++t)
+                    for (int k = 0; k < tc::tile_parts(dps[i].per_tile); ++k)
+                        items.push_back(tc::BatchItem{i, t, k});
     tc_batch *b = new (std::nothrow) tc_batch();
     if (!b) return fail(TC_ERR_ALLOC, "host allocation");
     b->lean = lean;

@@ -160,6 +160,9 @@ void plan_tiles(const int *rowptr, int M, const tc_params &prm, int min_tiles,
 // (40 registers: the stream tiles' words, terms and row pointers fit
 // without spills).
 constexpr int kLeanMinBlocks = 6, kLeanMinBlocksSigned = 6;
+// The same for the batch and served kernels, which read the plan descriptor
+// from memory instead of the parameter bank (48 registers).
+constexpr int kItemMinBlocks = 5;
 // Launch of the multiply kernel for one plan.
 tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
 tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,

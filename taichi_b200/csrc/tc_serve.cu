@@ -39,18 +39,19 @@ struct ReqDesc {
 
 constexpr int kMaxBatch = 256;
 
-// One CTA per tile of nreq requests whose matrices all have plain (SIGNED =
-// false) or all hybrid words; request i owns tiles [reqs[i].tile_begin,
-// reqs[i + 1].tile_begin) of the grid.  Thread 0 finds the CTA's request by
-// binary search and parks its plan descriptor in shared memory.  LEAN: every
-// admitted plan holds only stream, direct and long tiles.
+// One CTA per work item (tile, or quarter of a wide direct tile) of nreq
+// requests whose matrices all have plain (SIGNED = false) or all hybrid
+// words; request i owns items [reqs[i].tile_begin, reqs[i + 1].tile_begin)
+// of the grid.  Thread 0 finds the CTA's request by binary search and parks
+// its plan descriptor in shared memory.  LEAN: every admitted plan holds only
+// stream, direct and long tiles.
 template <bool SIGNED, bool LEAN>
-__global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned : kLeanMinBlocks) : 1)
+__global__ void __launch_bounds__(kBlock, LEAN ? kItemMinBlocks : 1)
     serve_kernel(const DevPlan *__restrict__ plans, const ReqDesc *__restrict__ reqs, int nreq)
 {
     __shared__ DevPlan sp;
     __shared__ ReqDesc sr;
-    __shared__ int stile;
+    __shared__ int sitem;
     const int g = blockIdx.x;
     if (threadIdx.x == 0) {
         int lo = 0, hi = nreq;                     // tile_begin[lo] <= g < tile_begin[hi]
@@ -60,12 +61,12 @@ __global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned 
         }
         sr = reqs[lo];
         sp = plans[sr.plan];
-        stile = g - sr.tile_begin;
+        sitem = g - sr.tile_begin;
     }
     __syncthreads();
-    const Tile t = sp.tiles[stile];
-    if (LEAN) run_lean_tile<SIGNED>(sp, t, sr.x, sr.y, false);
-    else run_tile<SIGNED>(sp, t, sr.x, sr.y, false);
+    const int parts = tile_parts(sp.per_tile);
+    const Tile t = sp.tiles[sitem / parts];
+    run_tile_part<SIGNED, LEAN>(sp, t, sitem % parts, sr.x, sr.y, false);
 }
 
 double now_s()
@@ -100,7 +101,7 @@ struct tc_server {
 };
 
 namespace {
-bool lean_plan(const tc_plan *p) { return p->dev_plan().per_tile == 2; }
+bool lean_plan(const tc_plan *p) { return p->dev_plan().per_tile >= 2; }
 }  // namespace
 
 namespace {
@@ -116,7 +117,7 @@ void tc_serve_config_default(tc_serve_config *c)
     if (!c) return;
     c->hbm_budget = 64LL << 30;
     c->arena_bytes = 256LL << 20;
-    c->contexts = 3;
+    c->contexts = 6;
     c->max_batch = 64;
     c->max_plans = 1024;
 }
@@ -293,7 +294,7 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
                     if (p->hybrid != pass) continue;
                     c.h_desc[k] = batch[i];
                     c.h_desc[k].tile_begin = tiles[pass];
-                    tiles[pass] += p->ntiles;
+                    tiles[pass] += p->ntiles * tc::tile_parts(p->dev_plan().per_tile);
                     c.reqs.push_back(order[i]);
                     np += pass == 0;
                     ++k;

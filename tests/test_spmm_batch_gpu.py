@@ -1,5 +1,7 @@
-"""SpMM (1..64 right-hand sides) and the batched persistent launch, against
-the FP64 oracle and against the single-plan multiply (bit-identical)."""
+"""SpMM (1..64 right-hand sides) and the batched launch over many plans,
+against the FP64 oracle and against the single-plan multiply
+(bit-identical, including plans of wide direct tiles, which the batch runs as
+quarter-tile work items)."""
 import numpy as np
 import pytest
 
@@ -57,14 +59,25 @@ def test_spmm_strided(tc, dev):
 def test_batch_identical_to_solo(tc, dev):
     import ctypes as C
     import torch
-    names = ["band_holes", "two_segments", "multi_shape", "cfg1_small", "wide_band", "overlap"]
+    names = ["band_holes", "two_segments", "multi_shape", "cfg1_small", "wide_band", "overlap",
+             "rmat16_selfloops", "plain:rmat16_selfloops", "plain:sparse"]
     plans, xs, ys, solo = [], [], [], []
     rng = np.random.default_rng(5)
     for nm in names:
-        case = next(c for c in cases.MATRIX_CASES if c["name"] == nm)
-        M, N, rp, col = cases.matrix(case)
-        fmt, _ = oracle.partition(M, N, rp, col)
-        p = tc.Plan.from_format(M, N, fmt)
+        if nm == "plain:sparse":             # rows of <= 1 entry on average: wide direct tiles
+            M = N = 9000
+            rp = np.zeros(M + 1, np.int32)
+            np.cumsum(rng.integers(0, 2, M), out=rp[1:])
+            col = rng.integers(0, N, int(rp[-1])).astype(np.int32)
+            p = tc.Plan.from_csr(M, N, rp, col, partition=False)
+        else:
+            case = next(c for c in cases.MATRIX_CASES if c["name"] == nm.split(":")[-1])
+            M, N, rp, col = cases.matrix(case)
+            if nm.startswith("plain:"):
+                p = tc.Plan.from_csr(M, N, rp, col, partition=False)
+            else:
+                fmt, _ = oracle.partition(M, N, rp, col)
+                p = tc.Plan.from_format(M, N, fmt)
         x = torch.from_numpy(rng.uniform(-1, 1, N).astype(np.float32)).to(dev)
         y = torch.empty(M, device=dev)
         p.spmv(x, y)
