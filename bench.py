@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from taichi_b200 import replicas  # noqa: E402  (plain Python; loads no CUDA library)
+
 METRIC = "SpMV GB/s (% of HBM peak) at R-MAT scale 20"
 L2_BYTES = 126 * 2 ** 20
 
@@ -233,8 +235,7 @@ def run_ours(args, rank, world, local_rank):
     clocks = Clocks(local_rank)
     clocks.start()
     time.sleep(0.3)
-    if world > 1:
-        torch.distributed.barrier()
+    replicas.barrier(world)
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -246,14 +247,10 @@ def run_ours(args, rank, world, local_rank):
             g_rem.replay()
         ev1.record(stream)
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    replicas.barrier(world)
     ms = ev0.elapsed_time(ev1)
     cl = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(ms, world, device=dev)    # the slowest replica bounds the job
     ms_step = ms / args.steps
     gbs = bytes_per / (ms_step * 1e-3) / 1e9 * world
     peak, peak_kind = load_peaks()
@@ -562,23 +559,15 @@ def main():
     if args.impl == "ours" and args.form != "plain":
         {"spmm": run_spmm, "batched": run_batched, "served": run_served}[args.form](args)
         return
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = replicas.env()
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, rank)           # rank 0 alone; no process group
         return
-    if world > 1:
-        import datetime
-        import torch
-        torch.cuda.set_device(local_rank)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rank, world, local_rank = replicas.init("nccl")
     try:
         run_ours(args, rank, world, local_rank)
     finally:
-        if world > 1:
-            import torch
-            torch.distributed.destroy_process_group()
+        replicas.finish(world)
 
 
 if __name__ == "__main__":
