@@ -144,6 +144,15 @@ TC_API tc_status tc_plan_thumbnail(const tc_plan *plan, unsigned char *stages, i
  * wait (its y is then incomplete); TC_OK otherwise.  Synchronous. */
 TC_API tc_status tc_plan_check(const tc_plan *plan);
 
+/* Plan files: the plan's TaiChi_new format and build parameters, so a matrix
+ * is partitioned once and reloaded later (a served pool restarts without
+ * repartitioning).  No counterpart in the reference, which repartitions on
+ * every run (TaiChi.cu:313-638).  tc_plan_load checks the file (magic, sizes,
+ * checksum: TC_ERR_FORMAT; unreadable: TC_ERR_IO) before it touches the GPU,
+ * then builds the plan with `params` (NULL: the saved parameters). */
+TC_API tc_status tc_plan_save(const tc_plan *plan, const char *path);
+TC_API tc_status tc_plan_load(const char *path, const tc_params *params, void *stream, tc_plan **out);
+
 /* y = A x.  d_x: N floats, d_y: M floats, device memory.  Stream-ordered. */
 TC_API tc_status tc_spmv(const tc_plan *plan, const float *d_x, float *d_y, void *stream);
 

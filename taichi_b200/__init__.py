@@ -59,7 +59,8 @@ class PlanInfo(C.Structure):
 EXPORTS = (
     "tc_params_default", "tc_last_error", "tc_status_string", "tc_plan_create",
     "tc_plan_from_format", "tc_plan_destroy", "tc_plan_info_get", "tc_plan_export",
-    "tc_plan_thumbnail", "tc_plan_check", "tc_spmv", "tc_spmv_host", "tc_spmv_host_async",
+    "tc_plan_thumbnail", "tc_plan_check", "tc_plan_save", "tc_plan_load", "tc_spmv", "tc_spmv_host",
+    "tc_spmv_host_async",
     "tc_spmm", "tc_getsdf",
     "tc_trace_contours", "tc_read_mtx", "tc_free", "tc_batch_create", "tc_batch_run",
     "tc_batch_graph_launch", "tc_batch_destroy", "tc_tune", "tc_tune_cache_clear",
@@ -95,6 +96,8 @@ def lib():
         L.tc_plan_export.argtypes = [vp] + [vp] * 7
         L.tc_plan_thumbnail.argtypes = [vp, vp, _IP, vp, _IP]
         L.tc_plan_check.argtypes = [vp]
+        L.tc_plan_save.argtypes = [vp, C.c_char_p]
+        L.tc_plan_load.argtypes = [C.c_char_p, C.POINTER(Params), vp, C.POINTER(vp)]
         L.tc_spmv.argtypes = [vp, vp, vp, vp]
         L.tc_spmv_host.argtypes = [vp, vp, vp, vp]
         L.tc_spmv_host_async.argtypes = [vp, vp, vp, C.c_int, vp]
@@ -401,6 +404,17 @@ class Plan:
     def check(self):
         """Raises if a multiply of this plan reported a device-side timeout."""
         check(lib().tc_plan_check(self._h))
+
+    # -- plan files ---------------------------------------------------------
+    def save(self, path):
+        check(lib().tc_plan_save(self._h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path, prm=None, stream=None):
+        h = C.c_void_p()
+        check(lib().tc_plan_load(os.fsencode(path), C.byref(prm) if prm is not None else None,
+                                 _stream(stream), C.byref(h)))
+        return cls(h)
 
     def spmv_host(self, x, y, stream=None):
         check(lib().tc_spmv_host(self._h, _ptr(x), _ptr(y), _stream(stream)))
