@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
             run_tile_src<SIGNED>(p, tile, src, x, y, !waited);
         }
         waited = true;
+        after_wait(x, y);                 // later tiles' x / y accesses follow the first tile's wait
         __syncthreads();                  // stage s is free again
         if (threadIdx.x == 0) {
             fence_async_shared();
@@ -271,7 +272,13 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
                                                                      float *__restrict__ y)
 {
     allow_next_grid();
-    direct_run<SIGNED>(p, p.tiles[blockIdx.x], x, y, true, 4 * threadIdx.x);
+    // wide tiles are laid out in order, kDirectWideRows rows each, so the
+    // rows are known without waiting for the tile record; only the diagonal
+    // class comes from it
+    const int row0 = blockIdx.x * kDirectWideRows, nr = min(kDirectWideRows, p.M - row0);
+    if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
+    const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+    direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
 }
 
 // The multiply of a stream plan: one CTA per tile, no shared-memory stages
@@ -284,6 +291,7 @@ __global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned 
 {
     allow_next_grid();
     const Tile t = p.tiles[blockIdx.x];
+    if (threadIdx.x == 0) prefetch_x_window(x, p.N, t.row0, tile_nrows(t));
     if (LEAN) {
         run_lean_tile<SIGNED>(p, t, x, y, true);
     } else {
@@ -529,6 +537,10 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     p->ntiles_lanes = 0;
     p->ntiles_wide = 0;
     for (const Tile &t : tiles) p->ntiles_wide += tile_kind(t) == TILE_DIRECT_WIDE;
+    // the direct kernel finds a wide tile's rows from its index
+    for (size_t i = 0; i < tiles.size() && p->ntiles_wide; ++i)
+        if (tiles[i].row0 != (int)i * kDirectWideRows || tile_kind(tiles[i]) != TILE_DIRECT_WIDE)
+            return fail(TC_ERR_FORMAT, "wide tile %d out of order", (int)i);
     for (const Tile &t : tiles) {
         p->ntiles_lanes += tile_kind(t) <= TILE_L32 || tile_kind(t) == TILE_MERGE;
         if (tile_nrows(t) < 1 || tile_nrows(t) > kMaxTileNrows)

@@ -276,3 +276,31 @@ def test_format_rejected(tc):
                row_start=0, row_stop=0, csrRow=rp, csrCol=np.full(10, 12, np.int32))
     with pytest.raises(tc.TcError):
         tc.Plan.from_format(M, N, bad)
+
+
+@pytest.mark.parametrize("name,mode", [("rmat16", 2), ("rmat16", 0), ("rmat16", 1), ("rmat20", 2),
+                                       ("rmat16_selfloops", 2), ("mesh128", 2), ("mesh128", 1)])
+def test_chained_multiplies(tc, dev, name, mode):
+    """Six multiplies back to back on one stream, each reading the vector the
+    one before wrote (v <- A v, as a power iteration does): the launches
+    overlap under programmatic dependent launch, and every gather must still
+    see its producer's writes.  Integer x keeps every value exact."""
+    import torch
+    if name.startswith("rmat"):
+        M, N, rp, col = matgen.rmat(int(name[4:6]), 16, 0.499, 0.001, 0.001, seed=3,
+                                    self_loops=name.endswith("selfloops"))
+    else:
+        M, N, rp, col = matgen.mesh9(grid=128, permute_frac=0.02, seed=5)
+    assert M == N
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(tile_mode=mode))
+    v0 = np.random.default_rng(11).integers(-2, 3, N).astype(np.float64)
+    bufs = [to_dev(v0.astype(np.float32), dev), torch.empty(N, dtype=torch.float32, device=dev)]
+    want = v0
+    for k in range(6):
+        plan.spmv(bufs[k & 1], bufs[(k + 1) & 1])
+        want = oracle.spmv_csr_f64(M, rp, col, want)
+    assert np.abs(want).max() < 2 ** 24
+    torch.cuda.synchronize()
+    plan.check()
+    np.testing.assert_array_equal(bufs[0].cpu().numpy().astype(np.float64), want)
+    plan.close()
