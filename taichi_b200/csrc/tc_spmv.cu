@@ -275,10 +275,13 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     // wide tiles are laid out in order, kDirectWideRows rows each, so the
     // rows are known without waiting for the tile record; only the diagonal
     // class comes from it
-    const int row0 = blockIdx.x * kDirectWideRows, nr = min(kDirectWideRows, p.M - row0);
-    if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
+    const int row0 = blockIdx.x * kDirectWideRows;
+    if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, kDirectWideRows);
     const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
-    direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
+    if (row0 + kDirectWideRows <= p.M && (reinterpret_cast<uintptr_t>(y) & 15) == 0)
+        direct_run_full<SIGNED>(p, dc, x, y, row0 + 4 * threadIdx.x);
+    else
+        direct_run<SIGNED>(p, row0, min(kDirectWideRows, p.M - row0), dc, x, y, true, 4 * threadIdx.x);
 }
 
 // The multiply of a stream plan: one CTA per tile, no shared-memory stages

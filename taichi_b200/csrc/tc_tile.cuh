@@ -650,6 +650,39 @@ __device__ __forceinline__ void direct_run(const DevPlan &p, int row0, int nr, i
     }
 }
 
+// The run of rows [g, g + 4) (g a multiple of 4, all four rows inside the
+// matrix, y 16-byte aligned): direct_run's terms and order without its edge
+// handling, for the full tiles of the direct kernel.
+template <bool SIGNED>
+__device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const float *__restrict__ x,
+                                                float *__restrict__ y, int g)
+{
+    const int4 r4 = __ldg(reinterpret_cast<const int4 *>(p.rowptr + g));
+    const int e4 = __ldg(p.rowptr + g + 4);
+    const int b[5] = {r4.x, r4.y, r4.z, r4.w, e4};
+    int c[kDirectW];
+#pragma unroll
+    for (int w = 0; w < kDirectW; ++w) c[w] = b[0] + w < e4 ? __ldg(p.cols + b[0] + w) : 0;
+    wait_prior_grid(x, y);
+    float v[kDirectW];
+#pragma unroll
+    for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if (SIGNED) diag_run4(p, x, dc, g, 4, acc);
+#pragma unroll
+    for (int w = 0; w < kDirectW; ++w)
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (b[0] + w >= b[u] && b[0] + w < b[u + 1]) acc[u] += v[w];
+    for (int j = b[0] + kDirectW; j < e4; ++j) {
+        const float z = gather<SIGNED>(x, __ldg(p.cols + j));
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (j >= b[u] && j < b[u + 1]) acc[u] += z;
+    }
+    *reinterpret_cast<float4 *>(y + g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+}
+
 template <bool SIGNED>
 __device__ __forceinline__ void direct_run(const DevPlan &p, const Tile &t, const float *__restrict__ x,
                                            float *__restrict__ y, bool wait, int g)
