@@ -267,7 +267,12 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
 // (A variant that read a per-run descriptor -- 4 packed row lengths and the
 // run's words padded to an int4, loaded together instead of row pointers then
 // words -- measured slower on R-MAT, 7.35 against 5.9 µs, and was dropped.)
-template <bool SIGNED>
+// FULL: every tile is whole (M a multiple of kDirectWideRows, N >= M) and x
+// and y are 16-byte aligned, so each run takes the edge-free path and the x
+// window is one aligned 16 KB prefetch; the launch picks it from those facts.
+// (One kernel holding both paths behind a per-tile branch ran the full tiles
+// 0.8 µs slower per R-MAT scale 20 multiply than this split.)
+template <bool SIGNED, bool FULL>
 __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan p, const float *__restrict__ x,
                                                                      float *__restrict__ y)
 {
@@ -276,12 +281,14 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     // rows are known without waiting for the tile record; only the diagonal
     // class comes from it
     const int row0 = blockIdx.x * kDirectWideRows;
-    if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, kDirectWideRows);
     const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
-    if (row0 + kDirectWideRows <= p.M && (reinterpret_cast<uintptr_t>(y) & 15) == 0)
+    if (FULL) {
+        if (threadIdx.x == 0) prefetch_l2(x + row0, kDirectWideRows * sizeof(float));
         direct_run_full<SIGNED>(p, dc, x, y, row0 + 4 * threadIdx.x);
-    else
+    } else {
+        if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, kDirectWideRows);
         direct_run<SIGNED>(p, row0, min(kDirectWideRows, p.M - row0), dc, x, y, true, 4 * threadIdx.x);
+    }
 }
 
 // The multiply of a stream plan: one CTA per tile, no shared-memory stages
@@ -439,7 +446,10 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
     attr[0].val.programmaticStreamSerializationAllowed = dp.pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED>, dp, x, y));
+    const bool full = dp.M % kDirectWideRows == 0 && dp.N >= dp.M &&
+                      ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+    if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
+    else if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, false>, dp, x, y));
     else if (dp.per_tile == 2) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, false>, dp, x, y));
     else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_tiles_kernel<SIGNED>, dp, x, y));

@@ -99,6 +99,13 @@ __device__ __forceinline__ void prefetch_x_window(const float *x, int N, int r0,
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
 }
 
+// One bulk L2 prefetch of [p, p + bytes): p 16-byte aligned, bytes a multiple
+// of 16, the whole range inside one allocation.
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll
