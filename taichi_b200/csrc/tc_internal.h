@@ -99,8 +99,9 @@ struct DevPlan {
     int stage_rp, stage_cw; // ints per shared-memory stage (row pointers, CSR words)
     int grid;               // persistent grid size
     int per_tile;           // one CTA per tile (stream plans): 1, or 2 when only stream,
-                            // direct and long tiles occur (the lean kernel), or 3 when
-                            // every tile is a wide direct tile (the direct kernel)
+                            // direct and long tiles occur (the lean kernel), 3 when
+                            // every tile is a wide direct tile (the direct kernel), or 4
+                            // when every tile is a stream tile (the stream kernel)
     int *err;               // device error word (1: a bounded wait gave up)
 };
 
@@ -127,6 +128,7 @@ struct tc_plan {
     int ntiles = 0, ntiles_vector = 0, ntiles_long = 0;
     int ntiles_lanes = 0;                // lane and merge tiles (TILE_L1..L32, TILE_MERGE)
     int ntiles_wide = 0;                 // TILE_DIRECT_WIDE tiles (all or none)
+    int ntiles_stream = 0;               // TILE_STREAM tiles
     int max_span = 0;
     int stage_rp = 8, stage_cw = 8, grid = 1;
     int *d_err = nullptr;
@@ -160,6 +162,12 @@ void plan_tiles(const int *rowptr, int M, const tc_params &prm, int min_tiles,
 // (40 registers: the stream tiles' words, terms and row pointers fit
 // without spills).
 constexpr int kLeanMinBlocks = 6, kLeanMinBlocksSigned = 6;
+// The stream-only kernel for plans of more tiles than one wave at that
+// occupancy: 8 CTAs per SM at 32 registers (no spills).  Many waves of tiles
+// gain from the extra resident loads (9-point mesh on 2048^2: 63.2 -> 52.5
+// µs); a single wave loses from the thinner threads (n = 65,536 random
+// matrix: 5.6 -> 6.7 µs), so a plan takes it only above one wave.
+constexpr int kStreamManyMinBlocks = 8;
 // The same for the batch and served kernels, which read the plan descriptor
 // from memory instead of the parameter bank (48 registers).
 constexpr int kItemMinBlocks = 5;

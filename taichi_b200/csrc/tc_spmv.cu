@@ -309,6 +309,20 @@ __global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned 
     }
 }
 
+// The multiply of a plan of stream tiles only (meshes, banded and other
+// matrices of short, even rows): the grid kernel with no code for the other
+// tile kinds.  MANY: more tiles than one wave, compiled for 8 CTAs per SM.
+template <bool SIGNED, bool MANY>
+__global__ void __launch_bounds__(kBlock, MANY ? kStreamManyMinBlocks
+                                               : (SIGNED ? kLeanMinBlocksSigned : kLeanMinBlocks))
+    spmv_stream_kernel(DevPlan p, const float *__restrict__ x, float *__restrict__ y)
+{
+    allow_next_grid();
+    const Tile t = p.tiles[blockIdx.x];
+    if (threadIdx.x == 0) prefetch_x_window(x, p.N, t.row0, tile_nrows(t));
+    tile_stream<SIGNED>(p, t, x, y, true);
+}
+
 // SpMM: a warp owns kRPW consecutive rows at a time; lane l holds columns
 // [l*V, l*V+V) of the k right-hand sides, so every X / Y row access is one
 // coalesced warp transaction.  The entries of the kRPW rows are walked in
@@ -450,6 +464,9 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
                       ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
     if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, false>, dp, x, y));
+    else if (dp.per_tile == 4 && dp.ntiles > kLeanMinBlocks * num_sms())
+        TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_stream_kernel<SIGNED, true>, dp, x, y));
+    else if (dp.per_tile == 4) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_stream_kernel<SIGNED, false>, dp, x, y));
     else if (dp.per_tile == 2) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_grid_kernel<SIGNED, false>, dp, x, y));
     else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_tiles_kernel<SIGNED>, dp, x, y));
@@ -503,7 +520,11 @@ tc::DevPlan tc_plan::dev_plan() const
     d.stage_rp = stage_rp;
     d.stage_cw = stage_cw;
     d.grid = grid;
-    d.per_tile = params.tile_mode != 2 ? 0 : ntiles_wide == ntiles && ntiles > 0 ? 3 : ntiles_lanes == 0 ? 2 : 1;
+    d.per_tile = params.tile_mode != 2 ? 0
+               : ntiles == 0 ? 2
+               : ntiles_wide == ntiles ? 3
+               : ntiles_stream == ntiles ? 4
+               : ntiles_lanes == 0 ? 2 : 1;
     d.err = d_err;
     return d;
 }
@@ -549,7 +570,11 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     plan_tiles(csrRow, M, p->params, 4 * num_sms(), tiles, &p->ntiles_vector, &p->ntiles_long);
     p->ntiles_lanes = 0;
     p->ntiles_wide = 0;
-    for (const Tile &t : tiles) p->ntiles_wide += tile_kind(t) == TILE_DIRECT_WIDE;
+    p->ntiles_stream = 0;
+    for (const Tile &t : tiles) {
+        p->ntiles_wide += tile_kind(t) == TILE_DIRECT_WIDE;
+        p->ntiles_stream += tile_kind(t) == TILE_STREAM;
+    }
     // the direct kernel finds a wide tile's rows from its index
     for (size_t i = 0; i < tiles.size() && p->ntiles_wide; ++i)
         if (tiles[i].row0 != (int)i * kDirectWideRows || tile_kind(tiles[i]) != TILE_DIRECT_WIDE)

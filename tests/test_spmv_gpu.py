@@ -279,7 +279,8 @@ def test_format_rejected(tc):
 
 
 @pytest.mark.parametrize("name,mode", [("rmat16", 2), ("rmat16", 0), ("rmat16", 1), ("rmat20", 2),
-                                       ("rmat16_selfloops", 2), ("mesh128", 2), ("mesh128", 1)])
+                                       ("rmat16_selfloops", 2), ("mesh128", 2), ("mesh128", 1),
+                                       ("mesh512", 2)])
 def test_chained_multiplies(tc, dev, name, mode):
     """Six multiplies back to back on one stream, each reading the vector the
     one before wrote (v <- A v, as a power iteration does): the launches
@@ -290,7 +291,7 @@ def test_chained_multiplies(tc, dev, name, mode):
         M, N, rp, col = matgen.rmat(int(name[4:6]), 16, 0.499, 0.001, 0.001, seed=3,
                                     self_loops=name.endswith("selfloops"))
     else:
-        M, N, rp, col = matgen.mesh9(grid=128, permute_frac=0.02, seed=5)
+        M, N, rp, col = matgen.mesh9(grid=int(name[4:]), permute_frac=0.02, seed=5)
     assert M == N
     plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(tile_mode=mode))
     v0 = np.random.default_rng(11).integers(-2, 3, N).astype(np.float64)
@@ -304,3 +305,24 @@ def test_chained_multiplies(tc, dev, name, mode):
     plan.check()
     np.testing.assert_array_equal(bufs[0].cpu().numpy().astype(np.float64), want)
     plan.close()
+
+
+def test_stream_kernel_many_tiles(tc, dev):
+    """Plans of stream tiles only, with more tiles than one wave at six CTAs
+    per SM, run the 8-CTA stream kernel: the hybrid plan (signed words) and
+    the plain CSR plan of the same mesh, both against the oracle."""
+    import torch
+    M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=9)
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    assert plan.info()["ntiles"] > 6 * sms
+    check_plan(plan, plan.export(), M, N, rp, col, dev, "stream/many")
+    x = np.random.default_rng(3).uniform(-1, 1, N).astype(np.float32)
+    y_many = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_csr(M, N, rp, col, partition=False)
+    y_plain = run_spmv(plan, x, M, dev)
+    plan.close()
+    y64 = oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64))
+    assert np.linalg.norm(y_many - y64) <= TOL * np.linalg.norm(y64)
+    assert np.linalg.norm(y_plain - y64) <= TOL * np.linalg.norm(y64)
