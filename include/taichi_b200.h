@@ -156,6 +156,11 @@ TC_API tc_status tc_plan_load(const char *path, const tc_params *params, void *s
 /* y = A x.  d_x: N floats, d_y: M floats, device memory.  Stream-ordered. */
 TC_API tc_status tc_spmv(const tc_plan *plan, const float *d_x, float *d_y, void *stream);
 
+/* The same multiply in double precision: d_x N doubles, d_y M doubles, device
+ * memory, stream-ordered, over the same plan.  Replaces the reference's
+ * VALUE_TYPE=double build of taichi_SpMV (TaiChi.h:62-64, TaiChi.cu:1331). */
+TC_API tc_status tc_spmv_f64(const tc_plan *plan, const double *d_x, double *d_y, void *stream);
+
 /* Same multiply on host buffers: copies x in, multiplies, copies y out and
  * waits.  Pinned host buffers give the full link bandwidth. */
 TC_API tc_status tc_spmv_host(const tc_plan *plan, const float *h_x, float *h_y, void *stream);

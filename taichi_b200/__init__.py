@@ -59,7 +59,7 @@ class PlanInfo(C.Structure):
 EXPORTS = (
     "tc_params_default", "tc_last_error", "tc_status_string", "tc_plan_create",
     "tc_plan_from_format", "tc_plan_destroy", "tc_plan_info_get", "tc_plan_export",
-    "tc_plan_thumbnail", "tc_plan_check", "tc_plan_save", "tc_plan_load", "tc_spmv", "tc_spmv_host",
+    "tc_plan_thumbnail", "tc_plan_check", "tc_plan_save", "tc_plan_load", "tc_spmv", "tc_spmv_f64", "tc_spmv_host",
     "tc_spmv_host_async",
     "tc_spmm", "tc_getsdf",
     "tc_trace_contours", "tc_read_mtx", "tc_free", "tc_batch_create", "tc_batch_run",
@@ -99,6 +99,7 @@ def lib():
         L.tc_plan_save.argtypes = [vp, C.c_char_p]
         L.tc_plan_load.argtypes = [C.c_char_p, C.POINTER(Params), vp, C.POINTER(vp)]
         L.tc_spmv.argtypes = [vp, vp, vp, vp]
+        L.tc_spmv_f64.argtypes = [vp, vp, vp, vp]
         L.tc_spmv_host.argtypes = [vp, vp, vp, vp]
         L.tc_spmv_host_async.argtypes = [vp, vp, vp, C.c_int, vp]
         L.tc_spmm.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_int, vp]
@@ -400,6 +401,10 @@ class Plan:
     # -- multiply -----------------------------------------------------------
     def spmv(self, x, y, stream=None):
         check(lib().tc_spmv(self._h, _ptr(x), _ptr(y), _stream(stream)))
+
+    def spmv_f64(self, x, y, stream=None):
+        """y = A x with float64 device vectors (x: N, y: M)."""
+        check(lib().tc_spmv_f64(self._h, _ptr(x), _ptr(y), _stream(stream)))
 
     def check(self):
         """Raises if a multiply of this plan reported a device-side timeout."""
