@@ -1,6 +1,6 @@
-"""The reference arm of bench.py on the CPU: one JSON line with the contract's
-keys on rank 0, nothing (and exit 0) on the other ranks of a multi-rank
-launch."""
+"""bench.py on the CPU: the reference arm prints one JSON line with the
+contract's keys on rank 0 and nothing (exit 0) on the other ranks of a
+multi-rank launch; the served form's rate bisection against a fake server."""
 import json
 import os
 import subprocess
@@ -36,3 +36,22 @@ def test_reference_arm_other_ranks_idle():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_refine_rate_bisection():
+    """The served form's rate search: a fake server whose p99 grows with the
+    rate (2 ms at 2,000 requests/s) and which serves every rate in full."""
+    sys.path.insert(0, ROOT)
+    import bench
+    calls = []
+
+    def p99_at(rate):
+        calls.append(rate)
+        return rate / 1000.0, rate
+
+    rate, tput = bench.refine_rate(p99_at, (1000.0, 1000.0), 4000.0, 6)
+    assert len(calls) == 6
+    assert 2000.0 - 3000.0 / 64 <= rate < 2000.0 and tput == rate
+    # nothing passes above the start: the start is kept
+    rate, tput = bench.refine_rate(lambda r: (5.0, r), (1000.0, 900.0), 4000.0, 3)
+    assert (rate, tput) == (1000.0, 900.0)
