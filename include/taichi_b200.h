@@ -141,7 +141,9 @@ TC_API tc_status tc_plan_thumbnail(const tc_plan *plan, unsigned char *stages, i
                             int *corners, int *ncorners);
 
 /* TC_ERR_TIMEOUT if a multiply of this plan gave up a bounded device-side
- * wait (its y is then incomplete); TC_OK otherwise.  Synchronous. */
+ * wait since the last check (its y is then incomplete); TC_OK otherwise.
+ * Reading the flag clears it, so each give-up is reported once.
+ * Synchronous. */
 TC_API tc_status tc_plan_check(const tc_plan *plan);
 
 /* Plan files: the plan's TaiChi_new format and build parameters, so a matrix
@@ -202,10 +204,14 @@ TC_API tc_status tc_getsdf(int M, int N, const int *d_rowptr, const int *d_col, 
  * The working images live in a fixed device array of the library (512 KB,
  * held on every GPU that loads the library until exit), so the thumbnail is
  * limited to height <= 512 and W <= 1024 (TC_ERR_CAPACITY beyond).  The first
- * call on a device looks up that array's address; make it before any stream
- * capture.  Calls share the array: calls that overlap on the GPU race.  *W
+ * call on a device (and the first after the device's context was destroyed,
+ * e.g. by cudaDeviceReset) looks up that array's address in the current
+ * context.  Every call reads a status word back into host memory and
+ * synchronizes `stream`, so no call may be made on a stream that is being
+ * captured.  Calls share the array: calls that overlap on the GPU race.  *W
  * receives the width (0 when the matrix is too small for a thumbnail, in
- * which case nothing is written).  Synchronizes `stream`. */
+ * which case nothing is written).  Parameters are range-checked as in
+ * tc_plan_create (TC_ERR_INVALID) before anything is launched. */
 TC_API tc_status tc_thumbnail_noalloc(int M, int N, const int *d_rowptr, const int *d_col,
                                       const tc_params *p, unsigned char *d_stages, int *W,
                                       void *stream);

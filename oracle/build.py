@@ -2,19 +2,19 @@
 
 * ``oracle/liboracle.so``: the C restatement in taichi_oracle.c (gcc, OpenMP).
 * ``oracle/_ref/libtaichi_ref.so``: the reference's own TaiChi.cu and mmio.cpp,
-  compiled unmodified from their sources under the reference checkout (default
-  /root/reference, or $TAICHI_REFERENCE) with the shim headers in
+  compiled unmodified from their sources under the reference checkout named by
+  the caller (argument, or $TAICHI_REFERENCE) with the shim headers in
   oracle/ref_shims and the bridge in oracle/ref_bridge.cpp.  Built only where
   the reference sources exist; the built library then travels with the tree.
 
-Run: ``python oracle/build.py`` (``--ref`` to require the reference build).
+Run: ``python oracle/build.py [--ref CHECKOUT]`` (TAICHI_REFERENCE=CHECKOUT
+works too; with neither, only the C restatement is built).
 """
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = os.environ.get("TAICHI_REFERENCE", "/root/reference")
 LIB = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_LIB = os.path.join(REF_DIR, "libtaichi_ref.so")
@@ -42,11 +42,15 @@ def build_oracle(force=False):
     return LIB
 
 
-def build_ref(force=False):
-    """Compile the reference's sources; returns the library path or None when
-    the reference checkout is absent."""
-    taichi_cu = os.path.join(REF_SRC, "TaiChi.cu")
-    mmio = os.path.join(REF_SRC, "mmio.cpp")
+def build_ref(ref_src=None, force=False):
+    """Compile the reference's sources from the checkout `ref_src` (default:
+    $TAICHI_REFERENCE); returns the library path, or the one built earlier,
+    or None when no checkout is named or it lacks the sources."""
+    ref_src = ref_src or os.environ.get("TAICHI_REFERENCE")
+    if not ref_src:
+        return REF_LIB if os.path.exists(REF_LIB) else None
+    taichi_cu = os.path.join(ref_src, "TaiChi.cu")
+    mmio = os.path.join(ref_src, "mmio.cpp")
     if not (os.path.exists(taichi_cu) and os.path.exists(mmio)):
         return REF_LIB if os.path.exists(REF_LIB) else None
     bridge = os.path.join(HERE, "ref_bridge.cpp")
@@ -57,7 +61,7 @@ def build_ref(force=False):
     os.makedirs(REF_DIR, exist_ok=True)
     objd = os.path.join(REF_DIR, "obj")
     os.makedirs(objd, exist_ok=True)
-    inc = ["-I", os.path.join(HERE, "ref_shims"), "-I", REF_SRC, "-I", HERE]
+    inc = ["-I", os.path.join(HERE, "ref_shims"), "-I", ref_src, "-I", HERE]
     # No -fopenmp: the shape loop's pragma is ignored, giving the sequential
     # (race-free) order of the reference's partition.
     nv = ["nvcc", "-O2", "-w", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
@@ -76,7 +80,8 @@ def build_ref(force=False):
 
 if __name__ == "__main__":
     print(build_oracle(force=True))
-    r = build_ref(force=True)
-    if r is None and "--ref" in sys.argv:
-        sys.exit("reference sources not found at %s" % REF_SRC)
+    src = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv[:-1] else None
+    r = build_ref(src, force=True)
+    if r is None and src:
+        sys.exit("reference sources (TaiChi.cu, mmio.cpp) not found under %s" % src)
     print(r)

@@ -71,7 +71,9 @@ void tc_params_default(tc_params *p)
     p->flags = 0;
 }
 
-static tc_status check_params(const tc_params &p)
+}  // extern "C"
+
+tc_status tc::check_params(const tc_params &p)
 {
     if (p.thumb_height < 2 || p.thumb_height > 4096)
         return fail(TC_ERR_INVALID, "thumb_height %d outside [2, 4096]", p.thumb_height);
@@ -88,6 +90,10 @@ static tc_status check_params(const tc_params &p)
         return fail(TC_ERR_INVALID, "max_lanes %d is not a power of two in [1, 32]", p.max_lanes);
     return TC_OK;
 }
+
+using tc::check_params;
+
+extern "C" {
 
 // Validates a host format and builds a plan from it.
 tc_status tc_plan_from_format(int M, int N, const tc_format *f, const tc_params *params,
@@ -222,7 +228,9 @@ tc_status tc_plan_check(const tc_plan *p)
     if (!p) return fail(TC_ERR_INVALID, "null plan");
     int e = 0;
     TC_CUDA(cudaMemcpy(&e, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    return e ? fail(TC_ERR_TIMEOUT, "a multiply of this plan gave up waiting for its staged tiles") : TC_OK;
+    if (!e) return TC_OK;
+    TC_CUDA(cudaMemset(p->d_err, 0, sizeof(int)));   // reported once: the next multiply starts clean
+    return fail(TC_ERR_TIMEOUT, "a multiply of this plan gave up waiting for its staged tiles");
 }
 
 tc_status tc_spmv(const tc_plan *p, const float *d_x, float *d_y, void *stream)

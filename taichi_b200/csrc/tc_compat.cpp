@@ -306,23 +306,36 @@ void taichi_SpMV(int M, int N, TaiChi_new *t, float *xHost, float *yHost)
         return;
     }
     cudaMemcpy(dx, xHost, sizeof(float) * (size_t)N, cudaMemcpyHostToDevice);
-    for (int i = 0; i < 10; ++i) tc_spmv(p, dx, dy, 0);
+    // every multiply's status is checked; the first failure is printed the way
+    // the reference prints a CUDA error (TaiChi.cu:42-55) and y is left as is
+    tc_status st = TC_OK;
+    for (int i = 0; i < 10 && st == TC_OK; ++i) st = tc_spmv(p, dx, dy, 0);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double total = 0.0;
-    for (int i = 0; i < nrun; ++i) {
+    for (int i = 0; i < nrun && st == TC_OK; ++i) {
         cudaEventRecord(e0, 0);
-        tc_spmv(p, dx, dy, 0);
+        st = tc_spmv(p, dx, dy, 0);
         cudaEventRecord(e1, 0);
         cudaEventSynchronize(e1);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         total += ms;
     }
-    if (nrun == 0) tc_spmv(p, dx, dy, 0);
+    if (nrun == 0 && st == TC_OK) st = tc_spmv(p, dx, dy, 0);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (st == TC_OK) st = tc_plan_check(p);     // a device-side give-up leaves y incomplete
+    if (st == TC_OK && cudaDeviceSynchronize() != cudaSuccess)
+        st = tc::fail(TC_ERR_CUDA, "multiply: %s", cudaGetErrorString(cudaGetLastError()));
+    if (st != TC_OK) {
+        printf("CUDA Runtime Error: %s\n", tc_last_error());
+        cudaFree(dx);
+        cudaFree(dy);
+        tc_plan_destroy(p);
+        return;
+    }
     printf("transfer_time:%.4f spmv_time=%.4f\n", tt / ntransfer, nrun ? total / nrun : 0.0);
     cudaMemcpy(yHost, dy, sizeof(float) * (size_t)M, cudaMemcpyDeviceToHost);
     cudaFree(dx);

@@ -32,6 +32,10 @@ tc_status fail(tc_status s, const char *fmt, ...);
 // at least `bytes` (never lowers it, so earlier launches stay valid).
 tc_status ensure_smem(const void *kernel, size_t bytes);
 
+// Range checks of a tc_params (partition constants and tile shape);
+// TC_ERR_INVALID with a message naming the field.
+tc_status check_params(const tc_params &p);
+
 #define TC_CHECK(st)                                                               \
     do {                                                                           \
         tc_status s_ = (st);                                                       \

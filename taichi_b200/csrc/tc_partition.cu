@@ -24,6 +24,7 @@
 //  5. assembly     per row: holes (shape, diagonal, row order) then unclaimed
 //                  entries in CSR order, with the sign bit.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,6 +35,7 @@
 #include <mutex>
 #include <vector>
 
+#include "tc_ctxcache.h"
 #include "tc_internal.h"
 #include "tc_scan.cuh"
 
@@ -1139,6 +1141,7 @@ extern "C" tc_status tc_getsdf(int M, int N, const int *d_rowptr, const int *d_c
     tc_params prm;
     tc_params_default(&prm);
     if (p) prm = *p;
+    TC_CHECK(tc::check_params(prm));
     tc::SdfOut o;
     TC_CHECK(tc::getsdf_device(M, N, d_rowptr, d_col, prm, stages != nullptr, (cudaStream_t)stream, o));
     *mF = o.mF;
@@ -1197,25 +1200,56 @@ constexpr int kNoAllocMaxH = 512, kNoAllocMaxW = 1024;
 constexpr int kNoAllocWords = 8 * kNoAllocMaxH * (kNoAllocMaxW / 32);
 static __device__ __align__(256) unsigned g_thumb_scratch[kNoAllocWords + 64];
 
-std::mutex g_noalloc_mu;
-unsigned *g_noalloc_addr[64] = {};
+ContextAddressCache<> g_noalloc_cache;
 
-// Device address of g_thumb_scratch on the current device (looked up once per
-// device; the host-side name is not a device address).
+// Id of the CUDA context current on this thread (0 when there is none yet or
+// the driver entry points are unavailable).  Read through the driver's entry
+// points, so the library does not link libcuda itself.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess && qb == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(a);
+            get_id = reinterpret_cast<GetId>(b);
+        }
+        (void)cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of g_thumb_scratch in the current context: looked up once
+// per device and context (the host-side name is not a device address, and a
+// context created after cudaDeviceReset gets a new lookup).
 tc_status noalloc_scratch(unsigned **out)
 {
     int dev = 0;
     TC_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return fail(TC_ERR_UNSUPPORTED, "device index %d", dev);
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_thumb_scratch);
-        if (e != cudaSuccess)
-            return fail(TC_ERR_CUDA, "cudaGetSymbolAddress(thumbnail scratch): %s", cudaGetErrorString(e));
-        g_noalloc_addr[dev] = static_cast<unsigned *>(p);
+    TC_CUDA(cudaSetDevice(dev));                 // initialises and makes current its primary context
+    void *p = nullptr;
+    cudaError_t err = cudaSuccess;
+    const int rc = g_noalloc_cache.get(dev, current_context_id(), [&](void **a) {
+        err = cudaGetSymbolAddress(a, g_thumb_scratch);
+        return err == cudaSuccess ? 0 : 1;
+    }, &p);
+    if (rc < 0) return fail(TC_ERR_UNSUPPORTED, "device index %d", dev);
+    if (rc != 0) {
+        (void)cudaGetLastError();
+        return fail(TC_ERR_CUDA, "cudaGetSymbolAddress(thumbnail scratch): %s", cudaGetErrorString(err));
     }
-    *out = g_noalloc_addr[dev];
+    *out = static_cast<unsigned *>(p);
     return TC_OK;
 }
 
@@ -1237,6 +1271,7 @@ extern "C" tc_status tc_thumbnail_noalloc(int M, int N, const int *d_rowptr, con
     tc_params p;
     tc_params_default(&p);
     if (params) p = *params;
+    TC_CHECK(tc::check_params(p));
     const int H = p.thumb_height;
     if (M <= H) return TC_OK;                      // no thumbnail (morohutils.cu:192-196)
     const int W = (int)((double)H / (double)M * N);

@@ -160,13 +160,30 @@ __device__ __forceinline__ bool mbar_test(uint64_t *m, unsigned parity)
                  " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_u32(m)), "r"(parity) : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after ~1 s of polling (the copies complete in
-// microseconds; a give-up is reported through the plan's error word).
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: gives up once kStageWaitNs of global-timer time have passed
+// since the first failed poll (the copies complete in microseconds; a
+// give-up is reported through the plan's error word).  The deadline is time,
+// not a poll count, because each try_wait may suspend the thread for a
+// hardware-chosen interval.
+constexpr uint64_t kStageWaitNs = 1000000000ull;   // 1 s
+
 __device__ __forceinline__ bool mbar_wait(uint64_t *m, unsigned parity)
 {
-    for (long i = 0; i < (1L << 22); ++i)
-        if (mbar_test(m, parity)) return true;
-    return false;
+    if (mbar_test(m, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        for (int i = 0; i < 32; ++i)
+            if (mbar_test(m, parity)) return true;
+        if (globaltimer_ns() - t0 > kStageWaitNs) return false;
+    }
 }
 __device__ __forceinline__ void fence_async_shared()
 {

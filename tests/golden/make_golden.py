@@ -166,7 +166,7 @@ def mtx():
 def main():
     obuild.build_oracle()
     if obuild.build_ref() is None:
-        sys.exit("the reference checkout is needed to build oracle/_ref")
+        sys.exit("set TAICHI_REFERENCE to the reference checkout to build oracle/_ref")
     os.makedirs(os.path.join(HERE, "mtx"), exist_ok=True)
     print("images ...")
     im = images()
