@@ -34,7 +34,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from taichi_b200 import replicas  # noqa: E402  (plain Python; loads no CUDA library)
+from taichi_b200 import replicas, workloads  # noqa: E402  (plain Python; loads no CUDA library)
 
 METRIC = "SpMV GB/s (% of HBM peak) at R-MAT scale 20"
 L2_BYTES = 126 * 2 ** 20
@@ -186,6 +186,10 @@ def run_ours(args, rank, world, local_rank):
         over["flags"] = tc.TC_FLAG_ROWS_STRIDED
     if args.no_direct:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_DIRECT
+    if args.no_window:
+        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_WINDOW
+    if args.window:
+        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WINDOW
     if args.tile_nnz is not None:
         over["tile_nnz"] = args.tile_nnz
     if args.ctas_per_sm is not None:
@@ -219,20 +223,36 @@ def run_ours(args, rank, world, local_rank):
             plans[i % ncopy].spmv(xs[i % ncopy], ys[i % ncopy], stream=stream)
     torch.cuda.synchronize()
 
-    # one graph of G back-to-back SpMVs over the copies, replayed `reps`
-    # times: exactly --steps multiplies (G = steps up to 4096, else the
-    # largest divisor of steps that is at most 4096)
-    G = graph_len(args.steps)
+    # The timed multiplies are captured in a CUDA graph and replayed on the
+    # device back to back.  Up to 8192 steps: one graph of LEAD untimed
+    # multiplies, an event, exactly --steps multiplies, an event (the events
+    # are graph nodes, so neither the host's graph submission nor the graph's
+    # start-up falls inside the timed span).  More steps: a graph of G
+    # multiplies (G the largest divisor of steps up to 4096) replayed
+    # steps / G times between two stream events, after one untimed replay
+    # that keeps the device busy while the host submits the timed ones.
+    LEAD = 16
+    in_graph = args.steps <= 8192
+    G = args.steps if in_graph else graph_len(args.steps)
     reps = args.steps // G
+    ev0 = torch.cuda.Event(enable_timing=True, external=in_graph)
+    ev1 = torch.cuda.Event(enable_timing=True, external=in_graph)
 
-    def capture(n):
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=stream):
-            for i in range(n):
-                plans[i % ncopy].spmv(xs[i % ncopy], ys[i % ncopy], stream=torch.cuda.current_stream())
-        return g
+    def spmv_i(i):
+        plans[i % ncopy].spmv(xs[i % ncopy], ys[i % ncopy], stream=torch.cuda.current_stream())
 
-    g_main = capture(G)
+    g_main = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g_main, stream=stream):
+        if in_graph:
+            for i in range(LEAD):
+                spmv_i(i)
+            ev0.record()
+            for i in range(args.steps):
+                spmv_i(LEAD + i)
+            ev1.record()
+        else:
+            for i in range(G):
+                spmv_i(i)
     with torch.cuda.stream(stream):
         g_main.replay()
     torch.cuda.synchronize()
@@ -242,16 +262,15 @@ def run_ours(args, rank, world, local_rank):
     time.sleep(0.3)
     replicas.barrier(world)
     torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):        # graph replays run on the current stream
-        # an untimed replay queued first keeps the device busy while the host
-        # submits the timed ones, so host submission latency is not timed
-        g_main.replay()
-        ev0.record(stream)
-        for _ in range(reps):
+        if in_graph:
             g_main.replay()
-        ev1.record(stream)
+        else:
+            g_main.replay()
+            ev0.record(stream)
+            for _ in range(reps):
+                g_main.replay()
+            ev1.record(stream)
     torch.cuda.synchronize()
     replicas.barrier(world)
     ms = ev0.elapsed_time(ev1)
@@ -262,6 +281,8 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = load_peaks()
 
     # warm-L2 figure (same copy every time) for context
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
     gw = torch.cuda.CUDAGraph()
     with torch.cuda.graph(gw, stream=stream):
         for _ in range(256):
@@ -330,6 +351,10 @@ def run_ours(args, rank, world, local_rank):
                        "tile_nnz": prm.tile_nnz, "flags": prm.flags,
                        "bytes_per_spmv": bytes_per, "format_build_s": round(build_s, 3),
                        "partition_ms": info["partition_ms"],
+                       "timing": ("one CUDA graph: %d untimed SpMVs, event, %d timed SpMVs, event "
+                                  "(events are graph nodes)" % (LEAD, args.steps) if in_graph else
+                                  "%d replays of a %d-SpMV graph after an untimed replay, stream events"
+                                  % (reps, G)),
                        "l2": "rotating %d resident copies (%.0f MB) > 2x L2" % (
                            ncopy, ncopy * bytes_per / 1e6),
                        "warm_l2_gbs": round(bytes_per / (warm_ms * 1e-3) / 1e9, 1),
@@ -345,6 +370,16 @@ def run_ours(args, rank, world, local_rank):
             "clocks": cl,
             "cpu_baseline": cpu,
         }
+        if world == 1 and not args.no_forms and not over and args.workload == "rmat20":
+            # the north star's other forms, each measured on its own workload
+            # with its own clocks record (GPU 0 only; replicas runs skip them)
+            for p in plans:
+                p.close()
+            plans = []
+            torch.cuda.empty_cache()
+            line["spmm"] = spmm_record(args)
+            line["batched"] = batched_record(args)
+            line["served"] = served_record(args)
         print(json.dumps(line), flush=True)
     for p in plans:
         p.close()
@@ -356,8 +391,10 @@ def _events(torch, stream):
     return a, b
 
 
-def run_spmm(args):
-    """Batched right-hand sides: Y = A X, X 4,194,304 x 64 FP32 (R-MAT scale 22)."""
+def spmm_record(args):
+    """Batched right-hand sides: Y = A X, X 4,194,304 x 64 FP32 row-major,
+    uniform in [-1, 1], A the R-MAT scale-22 graph (a = 0.499, b = c =
+    0.001, edge factor 16), formatted by the GPU partitioner."""
     import torch
     import taichi_b200 as tc
     dev = torch.device("cuda", 0)
@@ -365,69 +402,45 @@ def run_spmm(args):
     N, k = M, 64
     plan = tc.Plan.from_csr(M, N, rp, col)
     info = plan.info()
-    X = torch.empty((N, k), device=dev).uniform_(-1, 1)
+    X = torch.empty((N, k), device=dev).uniform_(-1, 1)       # 1 GiB, larger than L2
     Y = torch.empty((M, k), device=dev)
     stream = torch.cuda.Stream(dev)
     for _ in range(max(args.warmup, 3)):
         plan.spmm(X, Y, stream=stream)
     torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    time.sleep(0.2)
     a, b = _events(torch, stream)
-    steps = min(args.steps, 200)
+    steps = max(3, min(args.steps, 200))
     a.record(stream)
     for _ in range(steps):
         plan.spmm(X, Y, stream=stream)
     b.record(stream)
     torch.cuda.synchronize()
+    cl = clocks.stop()
     ms = a.elapsed_time(b) / steps
     nbytes = 4 * (M + 1) + 4 * info["nnz_csr"] + 4 * k * N + 4 * k * M
     peak, kind = load_peaks()
     gbs = nbytes / (ms * 1e-3) / 1e9
-    print(json.dumps({"form": "spmm", "metric": "SpMM GB/s (k=64) at R-MAT scale 22",
-                      "value": round(gbs, 1), "unit": "GB/s", "ms_per_step": ms, "steps": steps,
-                      "frac_of_hbm": round(gbs / peak, 4), "peak": peak, "peak_kind": kind,
-                      "config": {"M": M, "nnz": int(rp[M]), "k": k, "bytes": nbytes,
-                                 "dia_shapes": info["dia_shapes"]}}), flush=True)
+    plan.close()
+    return {"metric": "SpMM GB/s (k=64) at R-MAT scale 22", "value": round(gbs, 1), "unit": "GB/s",
+            "ms_per_step": ms, "steps": steps, "frac_of_hbm": round(gbs / peak, 4), "peak": peak,
+            "peak_kind": kind, "clocks": cl,
+            "config": {"workload": "rmat22_spmm_k64", "M": M, "nnz": int(rp[M]), "k": k,
+                       "bytes_per_spmm": nbytes, "dia_shapes": info["dia_shapes"],
+                       "l2": "X and Y are 1 GiB each, larger than L2"}}
 
 
-def pool_matrices(kind, count, seed):
-    """Seeded matrix pools of the batched (kind='batch') and served
-    (kind='serve') workloads."""
-    import taichi_b200 as tc
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(count):
-        if kind == "batch":
-            n = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
-            if i % 2 == 0:
-                sc = max(10, int(round(np.log2(n))))
-                M, rp, col = tc.gen_rmat(sc, 8, 0.499, 0.001, 0.001, seed=seed * 1000 + i)
-                out.append(("rmat%d" % sc, M, rp, col))
-            else:
-                kk = int(rng.integers(1, 17))
-                rp, col = tc.gen_banded(n, kk, 4, seed=seed * 1000 + i)
-                out.append(("band%d_k%d" % (n, kk), n, rp, col))
-        else:
-            if i < count // 2:
-                sc = 14 + (i * 9) // (count // 2)          # scales 14..22
-                M, rp, col = tc.gen_rmat(sc, 16, 0.499, 0.001, 0.001, seed=seed * 1000 + i)
-                out.append(("rmat%d" % sc, M, rp, col))
-            else:
-                n = int(np.exp(rng.uniform(np.log(1e4), np.log(4e6))))
-                kk = int(rng.integers(1, 17))
-                rr = int(rng.integers(2, 13))
-                rp, col = tc.gen_banded(n, kk, rr, seed=seed * 1000 + i)
-                out.append(("band%d_k%d_r%d" % (n, kk, rr), n, rp, col))
-    return out
-
-
-def run_batched(args):
-    """256 matrices of uneven size in one persistent, graph-captured launch,
-    autotuned per matrix, against one launch per matrix."""
+def batched_record(args):
+    """256 binary matrices of uneven size, each autotuned, multiplied by one
+    replay of a CUDA graph of the batch launch (one work list over every
+    matrix's tiles), against a graph of one launch per matrix."""
     import ctypes as C
     import torch
     import taichi_b200 as tc
     dev = torch.device("cuda", 0)
-    mats = pool_matrices("batch", 256, 7)
+    mats = workloads.pool_matrices("batch", 256, 7)
     t0 = time.perf_counter()
     plans, xs, ys, nbytes, tuned = [], [], [], 0, 0
     for name, M, rp, col in mats:
@@ -450,7 +463,10 @@ def run_batched(args):
     for _ in range(3):
         tc.check(tc.lib().tc_batch_graph_launch(b, C.c_void_p(stream.cuda_stream)))
     torch.cuda.synchronize()
-    steps = min(args.steps, 500)
+    steps = max(3, min(args.steps, 500))
+    clocks = Clocks(0)
+    clocks.start()
+    time.sleep(0.2)
     a, e = _events(torch, stream)
     a.record(stream)
     for _ in range(steps):
@@ -471,118 +487,116 @@ def run_batched(args):
             g.replay()
         e.record(stream)
     torch.cuda.synchronize()
+    cl = clocks.stop()
     ms_plain = a.elapsed_time(e) / steps
     tc.check(tc.lib().tc_batch_destroy(b))
-    print(json.dumps({"form": "batched", "matrices": n, "rows": int(sum(m[1] for m in mats)),
-                      "nnz": int(sum(int(m[2][-1]) for m in mats)),
-                      "batch_ms": ms_batch, "plain_ms": ms_plain,
-                      "batch_spmv_per_s": round(n / (ms_batch * 1e-3)),
-                      "plain_spmv_per_s": round(n / (ms_plain * 1e-3)),
-                      "batch_gbs": round(nbytes / (ms_batch * 1e-3) / 1e9, 1),
-                      "plain_gbs": round(nbytes / (ms_plain * 1e-3) / 1e9, 1),
-                      "speedup": round(ms_plain / ms_batch, 2), "tuned": tuned,
-                      "build_s": round(build_s, 1)}), flush=True)
+    del g
+    for p in plans:
+        p.close()
+    return {"metric": "SpMVs/s over 256 uneven matrices (one graph replay per batch)",
+            "matrices": n, "rows": int(sum(m[1] for m in mats)),
+            "nnz": int(sum(int(m[2][-1]) for m in mats)),
+            "batch_ms": ms_batch, "plain_ms": ms_plain,
+            "batch_spmv_per_s": round(n / (ms_batch * 1e-3)),
+            "plain_spmv_per_s": round(n / (ms_plain * 1e-3)),
+            "batch_gbs": round(nbytes / (ms_batch * 1e-3) / 1e9, 1),
+            "plain_gbs": round(nbytes / (ms_plain * 1e-3) / 1e9, 1),
+            "speedup": round(ms_plain / ms_batch, 2), "tuned": tuned, "tune_trials": args.tune_trials,
+            "build_s": round(build_s, 1), "steps": steps, "clocks": cl}
 
 
-def refine_rate(p99_at, lo, hi, steps, limit_ms=2.0):
-    """Bisection between a rate `lo` = (rate, spmv_per_s) whose p99 stayed
-    under limit_ms and a rate `hi` whose p99 did not: returns (rate,
-    spmv_per_s) of the highest passing rate found.  p99_at(rate) serves one
-    request stream at that rate and returns (p99_ms, spmv_per_s)."""
-    best = lo
-    a, b = lo[0], hi
-    for _ in range(steps):
-        mid = 0.5 * (a + b)
-        p99, tput = p99_at(mid)
-        if p99 < limit_ms:
-            a = mid
-            if tput > best[1]:
-                best = (mid, tput)
+def highest_passing_rate(serve_at, rates, bisect_steps, limit_ms=2.0):
+    """Sweeps `rates` (increasing) until a rate's p99 reaches limit_ms, then
+    bisects between the last passing and the first failing rate.
+    serve_at(rate) -> stats dict.  Returns (stats of the best passing run or
+    None, list of (rate, stats) of every run)."""
+    runs, best, fail = [], None, None
+    for rate in rates:
+        st = serve_at(rate)
+        runs.append((rate, st))
+        if st["p99_ms"] < limit_ms:
+            if best is None or st["spmv_per_s"] > best[1]["spmv_per_s"]:
+                best = (rate, st)
         else:
-            b = mid
-    return best
+            fail = rate
+            break
+    if best is not None and fail is not None and bisect_steps > 0:
+        a, b = best[0], fail
+        for _ in range(bisect_steps):
+            mid = 0.5 * (a + b)
+            st = serve_at(mid)
+            runs.append((mid, st))
+            if st["p99_ms"] < limit_ms:
+                a = mid
+                if st["spmv_per_s"] > best[1]["spmv_per_s"]:
+                    best = (mid, st)
+            else:
+                b = mid
+    return (best[1] if best else None), runs
 
 
-def run_served(args):
-    """Poisson arrivals, Zipf(1.1) over a 48-matrix resident pool; continuous
-    batching against one synchronous request at a time, with host vectors
-    (x copied in, y copied out per request) and with device vectors."""
+def served_record(args):
+    """Poisson arrivals of SpMV requests over a pool of 48 resident matrices
+    (Zipf(1.1) choice, a fresh x per request): the highest arrival rate whose
+    p99 latency stays under 2 ms, for continuous batching (online submit,
+    server-side dispatcher) and for the plain form (one synchronous request
+    at a time), with device vectors and with host vectors."""
     import torch
     import taichi_b200 as tc
     dev = torch.device("cuda", 0)
-    mats = pool_matrices("serve", 48, 11)
-    srv = tc.Server(contexts=args.serve_contexts, max_batch=args.serve_max_batch, arena_bytes=512 << 20,
-                    hbm_budget=96 << 30)
+    mats = workloads.pool_matrices("serve", 48, 11)
+    srv = tc.Server(contexts=args.serve_contexts, max_batch=args.serve_max_batch,
+                    max_inflight=args.serve_inflight, arena_bytes=512 << 20, hbm_budget=96 << 30)
     plans, ids = [], []
     for name, M, rp, col in mats:
         p = tc.Plan.from_csr(M, M, rp, col)
         plans.append(p)
         ids.append(srv.admit(p))
     rng = np.random.default_rng(5)
-    # two x and y buffers per matrix, reused round-robin
-    xb = [[torch.empty(m[1]).uniform_(-1, 1).pin_memory() for _ in range(2)] for m in mats]
-    yb = [[torch.empty(m[1]).pin_memory() for _ in range(2)] for m in mats]
-    xd = [[x.to(dev) for x in pair] for pair in xb]
-    yd = [[torch.empty(m[1], device=dev) for _ in range(2)] for m in mats]
-    ranks = np.arange(1, len(mats) + 1, dtype=np.float64)
-    pz = ranks ** -1.1
+    pz = np.arange(1, len(mats) + 1, dtype=np.float64) ** -1.1
     pz /= pz.sum()
+    # two x per matrix; enough y per matrix that requests in flight together
+    # never share one (at most max_inflight * max_batch are in flight)
+    in_flight = args.serve_inflight * args.serve_max_batch
+    nbuf = [int(np.ceil(2 * pz[m] * in_flight)) + 2 for m in range(len(mats))]
+    xh = [[torch.empty(m[1]).uniform_(-1, 1).pin_memory() for _ in range(2)] for m in mats]
+    yh = [[torch.empty(m[1]).pin_memory() for _ in range(nbuf[i])] for i, m in enumerate(mats)]
+    xd = [[x.to(dev) for x in pair] for pair in xh]
+    yd = [[torch.empty(m[1], device=dev) for _ in range(nbuf[i])] for i, m in enumerate(mats)]
     nreq = args.requests
-    forms = (("host", 0, args.rates, xb, yb),
-             ("device", tc.SERVE_DEVICE_VECTORS, args.device_rates, xd, yd))
-    summary = {}
-    for form, bit, rates, XB, YB in forms:
-        results = []
-        for rate in rates:
-            matrix = rng.choice(len(mats), size=nreq, p=pz)
-            arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
-            xs = [XB[m][i & 1] for i, m in enumerate(matrix)]
-            ys = [YB[m][i & 1] for i, m in enumerate(matrix)]
-            row = {"vectors": form, "rate": rate}
-            for mode, name in ((0, "batched"), (1, "plain")):
-                st, lat = srv.run(arrival, [ids[m] for m in matrix], xs, ys, mode=mode | bit)
-                row[name] = {k: round(st[k], 4) for k in ("spmv_per_s", "p50_ms", "p99_ms", "mean_batch")}
-            results.append(row)
-            print(json.dumps(row), flush=True)
-
-        def best(name):   # highest served rate whose p99 stays under 2 ms
-            ok = [r[name]["spmv_per_s"] for r in results if r[name]["p99_ms"] < 2.0]
-            return max(ok) if ok else 0.0
-        b, pl = best("batched"), best("plain")
-        summary[form] = {"batched_spmv_per_s_p99_lt_2ms": b, "plain_spmv_per_s_p99_lt_2ms": pl,
-                         "ratio": round(b / pl, 2) if pl else None, "results": results}
-        if args.rate_search > 0:
-            # the swept rate list is coarse: bisect each form's last passing
-            # and first failing rate
-            refined = {}
-            for mode, name in ((0, "batched"), (1, "plain")):
-                ok = [r for r in results if r[name]["p99_ms"] < 2.0]
-                if not ok:
-                    continue
-                lo = max(ok, key=lambda r: r[name]["spmv_per_s"])
-                bad = [r["rate"] for r in results if r[name]["p99_ms"] >= 2.0 and r["rate"] > lo["rate"]]
-                if not bad:
-                    refined[name] = lo[name]["spmv_per_s"]
-                    continue
-
-                def p99_at(rate, mode=mode):
-                    matrix = rng.choice(len(mats), size=nreq, p=pz)
-                    arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
-                    xs = [XB[m][i & 1] for i, m in enumerate(matrix)]
-                    ys = [YB[m][i & 1] for i, m in enumerate(matrix)]
-                    st, _ = srv.run(arrival, [ids[m] for m in matrix], xs, ys, mode=mode | bit)
-                    return st["p99_ms"], st["spmv_per_s"]
-                refined[name] = refine_rate(p99_at, (lo["rate"], lo[name]["spmv_per_s"]), min(bad),
-                                            args.rate_search)[1]
-            if "batched" in refined and refined.get("plain"):
-                summary[form]["refined"] = {"batched_spmv_per_s_p99_lt_2ms": round(refined["batched"], 1),
-                                            "plain_spmv_per_s_p99_lt_2ms": round(refined["plain"], 1),
-                                            "ratio": round(refined["batched"] / refined["plain"], 2),
-                                            "bisection_steps": args.rate_search}
-    print(json.dumps({"form": "served", "requests": nreq, "pool": len(mats),
-                      "pool_rows": int(sum(m[1] for m in mats)), "contexts": args.serve_contexts,
-                      "max_batch": args.serve_max_batch, "summary": summary}), flush=True)
+    keys = ("spmv_per_s", "p50_ms", "p99_ms", "mean_batch")
+    out = {"requests": nreq, "pool": len(mats), "pool_rows": int(sum(m[1] for m in mats)),
+           "contexts": args.serve_contexts, "max_batch": args.serve_max_batch,
+           "max_inflight": args.serve_inflight, "bisection_steps": args.rate_search}
+    clocks = Clocks(0)
+    clocks.start()
+    for form, bit, rates, XB, YB in (("device", tc.SERVE_DEVICE_VECTORS, args.device_rates, xd, yd),
+                                     ("host", 0, args.rates, xh, yh)):
+        rec = {}
+        for mode, name in ((0, "batched"), (1, "plain")):
+            def serve_at(rate, mode=mode):
+                matrix = rng.choice(len(mats), size=nreq, p=pz)
+                arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
+                cnt = np.zeros(len(mats), np.int64)
+                xs, ys = [], []
+                for i, m in enumerate(matrix):
+                    xs.append(XB[m][i & 1])
+                    ys.append(YB[m][cnt[m] % nbuf[m]])
+                    cnt[m] += 1
+                st, _ = srv.run(arrival, [ids[m] for m in matrix], xs, ys, mode=mode | bit)
+                return st
+            best, runs = highest_passing_rate(serve_at, rates, args.rate_search)
+            rec[name] = dict({k: round(best[k], 4) for k in keys} if best else {"spmv_per_s": 0.0},
+                             runs=[[round(r, 1)] + [round(st[k], 4) for k in keys] for r, st in runs])
+        pl = rec["plain"]["spmv_per_s"]
+        rec["ratio"] = round(rec["batched"]["spmv_per_s"] / pl, 2) if pl else None
+        out[form] = rec
+    out["clocks"] = clocks.stop()
+    out["runs_columns"] = ["rate"] + list(keys)
     srv.close()
+    for p in plans:
+        p.close()
+    return out
 
 
 def main():
@@ -592,12 +606,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat20")
-    ap.add_argument("--form", default="plain", choices=["plain", "spmm", "batched", "served"])
-    ap.add_argument("--tune-trials", type=int, default=8)
-    ap.add_argument("--requests", type=int, default=20000)
-    ap.add_argument("--rates", type=float, nargs="+", default=[2000, 5000, 10000, 15000, 20000, 40000])
+    ap.add_argument("--form", default="plain", choices=["plain", "spmm", "batched", "served"],
+                    help="plain: the headline line (with the spmm, batched and served records "
+                         "unless --no-forms); others: that record alone")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain line only, without the spmm / batched / served records")
+    ap.add_argument("--tune-trials", type=int, default=4, help="batched form: tuner trials per matrix")
+    ap.add_argument("--requests", type=int, default=20000, help="served form: requests per rate")
+    ap.add_argument("--rates", type=float, nargs="+",
+                    default=[2000, 4000, 6000, 9000, 13500, 20000, 30000, 45000, 67500, 100000],
+                    help="served form, host vectors: arrival rates swept (requests/s)")
     ap.add_argument("--device-rates", type=float, nargs="+",
-                    default=[20000, 40000, 50000, 60000, 100000, 125000, 150000, 175000, 200000])
+                    default=[20000, 30000, 45000, 67500, 100000, 150000, 225000, 337500, 506250,
+                             759375, 1139062],
+                    help="served form, device vectors: arrival rates swept (requests/s)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tile-mode", type=int, default=None, help="0 merge, 1 lanes, 2 stream")
@@ -606,13 +628,17 @@ def main():
     ap.add_argument("--tile-nnz", type=int, default=None, help="entry limit of a tile")
     ap.add_argument("--ctas-per-sm", type=int, default=None, help="resident CTAs per SM (persistent grids)")
     ap.add_argument("--no-direct", action="store_true", help="stream tiles only, no direct tiles")
-    ap.add_argument("--serve-contexts", type=int, default=6, help="served form: launch contexts in flight")
+    ap.add_argument("--no-window", action="store_true", help="never the window kernel")
+    ap.add_argument("--window", action="store_true", help="the window kernel wherever rows fit its tiles")
+    ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")
     ap.add_argument("--serve-max-batch", type=int, default=64, help="served form: most requests per launch")
-    ap.add_argument("--rate-search", type=int, default=0,
+    ap.add_argument("--serve-inflight", type=int, default=2, help="served form: batches on the GPU at once")
+    ap.add_argument("--rate-search", type=int, default=4,
                     help="served form: bisection steps between the last passing and first failing rate")
     args = ap.parse_args()
     if args.impl == "ours" and args.form != "plain":
-        {"spmm": run_spmm, "batched": run_batched, "served": run_served}[args.form](args)
+        rec = {"spmm": spmm_record, "batched": batched_record, "served": served_record}[args.form](args)
+        print(json.dumps(dict(form=args.form, **rec)), flush=True)
         return
     rank, world, local_rank = replicas.env()
     if args.impl == "reference":

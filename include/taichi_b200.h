@@ -75,6 +75,12 @@ typedef struct tc_params {
 #define TC_FLAG_NO_WIDE      0x20 /* tile_mode 2: no wide direct tiles (a
                                      1024-thread CTA per 4096 rows) for a
                                      matrix whose rows all qualify          */
+#define TC_FLAG_NO_WINDOW    0x40 /* tile_mode 2: never run the window kernel
+                                     (x staged in shared memory per tile of
+                                     rows), even for a banded matrix        */
+#define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
+                                     whenever the rows fit its tiles, even
+                                     where the planner would not choose it   */
 
 TC_API void tc_params_default(tc_params *p);
 
@@ -124,6 +130,9 @@ typedef struct tc_plan_info {
     int64_t spmv_bytes;       /* algorithmic bytes of one SpMV                */
     double partition_ms;      /* GPU partition time at creation               */
     int num_contours;         /* thumbnail contours kept (>= min_contour)      */
+    int nwtiles;              /* window tiles (0: the plan has no window plan) */
+    int window_lo, window_hi; /* x window of rows [r0, r0+n):
+                                 [r0 + window_lo, r0 + n + window_hi)          */
 } tc_plan_info;
 
 TC_API tc_status tc_plan_info_get(const tc_plan *plan, tc_plan_info *info);
@@ -235,6 +244,20 @@ TC_API tc_status tc_read_mtx(const char *path, int *M, int *N, int64_t *nnz, int
                       int **col, float **val, int *ref_code);
 TC_API void tc_free(void *p);
 
+/* The same file with the CSR built on the GPU: the text is parsed on the
+ * host (as tc_read_mtx), the entries are copied to the device once, and a
+ * stable radix sort by row puts them in readMtx's order (file order within
+ * each row, a symmetric file's mirror right after its entry's step) --
+ * replacing the host counting sort of readMtx (TaiChi.cu:170-270).  The
+ * arrays are device memory (free each with tc_device_free) and can go
+ * straight to tc_plan_create with on_device = 1.  *parse_ms / *build_ms
+ * (optional) receive the host parse and the device build times.
+ * Synchronizes `stream`. */
+TC_API tc_status tc_read_mtx_device(const char *path, int *M, int *N, int64_t *nnz, int **d_rowptr,
+                                    int **d_col, float **d_val, int *ref_code, double *parse_ms,
+                                    double *build_ms, void *stream);
+TC_API void tc_device_free(void *p);
+
 /* Synthetic benchmark matrices (no counterpart in the reference, whose
  * datasets are external files): R-MAT graphs (each of ef * 2^scale edges
  * picks a quadrant per level with probabilities a, b, c, 1-a-b-c) and
@@ -289,9 +312,13 @@ typedef struct tc_server tc_server;
 typedef struct tc_serve_config {
     int64_t hbm_budget;   /* bytes for admitted plans + request arenas (64 GiB)    */
     int64_t arena_bytes;  /* device x / y space of one launch context (256 MiB)   */
-    int contexts;         /* launch contexts (streams) in flight (6)             */
-    int max_batch;        /* most requests packed into one launch (64, <= 256)   */
+    int contexts;         /* launch contexts (streams) (4)                       */
+    int max_batch;        /* most requests packed into one launch (64, <= 128)   */
     int max_plans;        /* size of the resident plan table (1024)              */
+    int max_inflight;     /* batches on the GPU at once, <= contexts (2): a new
+                             batch launches when fewer are in flight, with every
+                             request waiting by then                            */
+    int max_pending;      /* online requests outstanding at once (65536)         */
 } tc_serve_config;
 
 typedef struct tc_serve_stats {
@@ -306,24 +333,48 @@ TC_API void tc_serve_config_default(tc_serve_config *c);
 TC_API tc_status tc_server_create(const tc_serve_config *c, tc_server **out);
 /* Makes `plan` resident in the server (not owned; keep it alive).  Returns
  * TC_ERR_CAPACITY when its HBM footprint does not fit the budget left, or its
- * x and y do not fit an arena. */
+ * x and y do not fit an arena.  While the server is started, admission reuses
+ * the slots of evicted matrices only (TC_ERR_UNSUPPORTED otherwise). */
 TC_API tc_status tc_server_admit(tc_server *s, tc_plan *plan, int *matrix_id);
+/* TC_ERR_CAPACITY while requests for the matrix are queued or running. */
 TC_API tc_status tc_server_evict(tc_server *s, int matrix_id);
 TC_API int64_t tc_server_hbm_used(const tc_server *s);
+
+/* Online serving.  tc_server_start launches the server's dispatcher thread:
+ * it batches the submitted requests continuously (a batch launches whenever
+ * fewer than max_inflight are on the GPU, with every request waiting by then,
+ * up to max_batch).  device_vectors != 0: requests carry device x / y that
+ * the caller owns (requests in flight together must not share a y); 0: host
+ * x / y (pinned memory gives full copy bandwidth), copied through the
+ * contexts' arenas.  tc_server_submit may be called from any thread; it
+ * returns a ticket for tc_server_poll (non-blocking: *done = 1 once y is
+ * complete) or tc_server_wait (blocking, timeout in seconds, < 0: none;
+ * TC_ERR_TIMEOUT when it runs out).  A failed batch fails its requests with
+ * the dispatcher's status.  tc_server_stats covers the requests completed
+ * since the start (latency = completion - submission).  tc_server_stop
+ * serves what was submitted, then stops the thread. */
+TC_API tc_status tc_server_start(tc_server *s, int device_vectors);
+TC_API tc_status tc_server_submit(tc_server *s, int matrix_id, const float *x, float *y,
+                                  uint64_t *ticket);
+TC_API tc_status tc_server_poll(tc_server *s, uint64_t ticket, int *done);
+TC_API tc_status tc_server_wait(tc_server *s, uint64_t ticket, double timeout_s);
+TC_API tc_status tc_server_stats(tc_server *s, tc_serve_stats *stats);
+TC_API tc_status tc_server_stop(tc_server *s);
+
 /* Serves a request trace in real time: request r arrives arrival_s[r]
  * seconds after the call starts (non-decreasing), multiplies matrix[r] by the
- * host vector h_x[r] and leaves y in h_y[r] (pinned host memory gives full
- * copy bandwidth).  mode 0: continuous batching; mode 1: one synchronous
- * request at a time (the plain form).  With TC_SERVE_DEVICE_VECTORS added to
- * the mode, h_x[r] / h_y[r] are device vectors owned by the caller: nothing is
- * copied, a batch is one launch over its requests' tiles and the plain form
- * is one synchronous tc_spmv per request (requests in flight together must
- * not share a y).  latency_ms[r] (optional) receives completion minus
- * arrival. */
+ * host vector h_x[r] and leaves y in h_y[r].  mode 0: continuous batching
+ * (the online path above, each request submitted at its arrival time); mode
+ * 1: one synchronous request at a time on the calling thread (the plain
+ * form).  With TC_SERVE_DEVICE_VECTORS added to the mode, h_x[r] / h_y[r] are
+ * device vectors owned by the caller: nothing is copied, and the plain form
+ * is one synchronous tc_spmv per request.  latency_ms[r] (optional) receives
+ * completion minus arrival.  Not while the server is started. */
 #define TC_SERVE_DEVICE_VECTORS 2
 TC_API tc_status tc_server_run(tc_server *s, int nreq, const double *arrival_s, const int *matrix,
                                const float *const *h_x, float *const *h_y, int mode,
                                double *latency_ms, tc_serve_stats *stats);
+/* Stops the server if started, then frees it. */
 TC_API tc_status tc_server_destroy(tc_server *s);
 
 #ifdef __cplusplus

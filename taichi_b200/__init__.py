@@ -22,6 +22,8 @@ TC_FLAG_NO_PDL = 0x4
 TC_FLAG_ROWS_STRIDED = 0x8
 TC_FLAG_NO_DIRECT = 0x10
 TC_FLAG_NO_WIDE = 0x20
+TC_FLAG_NO_WINDOW = 0x40
+TC_FLAG_WINDOW = 0x80
 
 _IP = C.POINTER(C.c_int)
 
@@ -52,7 +54,8 @@ class PlanInfo(C.Structure):
                 ("row_start", C.c_int), ("row_stop", C.c_int), ("nnz_input", C.c_int64),
                 ("nnz_csr", C.c_int64), ("ntiles", C.c_int), ("ntiles_vector", C.c_int),
                 ("ntiles_long", C.c_int), ("device_bytes", C.c_int64), ("spmv_bytes", C.c_int64),
-                ("partition_ms", C.c_double), ("num_contours", C.c_int)]
+                ("partition_ms", C.c_double), ("num_contours", C.c_int), ("nwtiles", C.c_int),
+                ("window_lo", C.c_int), ("window_hi", C.c_int)]
 
 
 # extern "C" symbols declared in include/taichi_b200.h (checked by the tests)
@@ -66,6 +69,8 @@ EXPORTS = (
     "tc_batch_graph_launch", "tc_batch_destroy", "tc_tune", "tc_tune_cache_clear",
     "tc_serve_config_default", "tc_server_create", "tc_server_admit", "tc_server_evict",
     "tc_server_hbm_used", "tc_server_run", "tc_server_destroy", "tc_thumbnail_noalloc",
+    "tc_server_start", "tc_server_submit", "tc_server_poll", "tc_server_wait", "tc_server_stats",
+    "tc_server_stop", "tc_read_mtx_device", "tc_device_free",
 )
 
 
@@ -111,6 +116,11 @@ def lib():
         L.tc_read_mtx.argtypes = [C.c_char_p, _IP, _IP, C.POINTER(C.c_int64), C.POINTER(_IP),
                                   C.POINTER(_IP), C.POINTER(C.POINTER(C.c_float)), _IP]
         L.tc_free.argtypes = [vp]
+        L.tc_read_mtx_device.argtypes = [C.c_char_p, _IP, _IP, C.POINTER(C.c_int64), C.POINTER(vp),
+                                         C.POINTER(vp), C.POINTER(vp), _IP, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), vp]
+        L.tc_device_free.argtypes = [vp]
+        L.tc_device_free.restype = None
         L.tc_gen_rmat.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                   C.c_uint64, C.c_int, _IP, C.POINTER(_IP), C.POINTER(_IP)]
         L.tc_gen_banded.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_IP),
@@ -133,6 +143,12 @@ def lib():
         L.tc_server_run.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp,
                                     C.POINTER(ServeStats)]
         L.tc_server_destroy.argtypes = [vp]
+        L.tc_server_start.argtypes = [vp, C.c_int]
+        L.tc_server_submit.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_uint64)]
+        L.tc_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(C.c_int)]
+        L.tc_server_wait.argtypes = [vp, C.c_uint64, C.c_double]
+        L.tc_server_stats.argtypes = [vp, C.POINTER(ServeStats)]
+        L.tc_server_stop.argtypes = [vp]
         _LIB = L
     return _LIB
 
@@ -175,7 +191,8 @@ def _stream(s):
 
 class ServeConfig(C.Structure):
     _fields_ = [("hbm_budget", C.c_int64), ("arena_bytes", C.c_int64), ("contexts", C.c_int),
-                ("max_batch", C.c_int), ("max_plans", C.c_int)]
+                ("max_batch", C.c_int), ("max_plans", C.c_int), ("max_inflight", C.c_int),
+                ("max_pending", C.c_int)]
 
 
 class ServeStats(C.Structure):
@@ -228,6 +245,33 @@ class Server:
                                   lat.ctypes.data, C.byref(st)))
         return {k: getattr(st, k) for k, _ in ServeStats._fields_}, lat
 
+    # -- online requests (tc_server_start / submit / poll / wait / stop) ----
+    def start(self, device_vectors=True):
+        check(lib().tc_server_start(self._h, 1 if device_vectors else 0))
+
+    def submit(self, mid, x, y):
+        """Queues y = A_mid x; returns a ticket (x / y: device tensors after
+        start(device_vectors=True), pinned host tensors otherwise)."""
+        t = C.c_uint64()
+        check(lib().tc_server_submit(self._h, mid, _ptr(x), _ptr(y), C.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        d = C.c_int()
+        check(lib().tc_server_poll(self._h, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket, timeout_s=-1.0):
+        check(lib().tc_server_wait(self._h, ticket, timeout_s))
+
+    def stats(self):
+        st = ServeStats()
+        check(lib().tc_server_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+    def stop(self):
+        check(lib().tc_server_stop(self._h))
+
     def close(self):
         if self._h:
             lib().tc_server_destroy(self._h)
@@ -275,6 +319,34 @@ def gen_banded(n, k, per_row, seed):
     rp, ci = _IP(), _IP()
     check(lib().tc_gen_banded(n, k, per_row, seed, C.byref(rp), C.byref(ci)))
     return _take_csr(n, rp, ci)
+
+
+def read_mtx_device(path, stream=None):
+    """Matrix Market -> CSR built on the GPU (tc_read_mtx_device).  Returns
+    ((M, N, rowptr, col, val), (parse_ms, build_ms)) with rowptr / col / val
+    as torch CUDA tensors (copied from the library's arrays, which are then
+    freed)."""
+    import torch
+    L = lib()
+    M, N, nnz, code = C.c_int(), C.c_int(), C.c_int64(), C.c_int()
+    ptrs = [C.c_void_p(), C.c_void_p(), C.c_void_p()]
+    pm, bm = C.c_double(), C.c_double()
+    st = L.tc_read_mtx_device(path.encode(), C.byref(M), C.byref(N), C.byref(nnz), C.byref(ptrs[0]),
+                              C.byref(ptrs[1]), C.byref(ptrs[2]), C.byref(code), C.byref(pm), C.byref(bm),
+                              _stream(stream))
+    if st != 0:
+        raise TcError(st, "%s (reference code %d)" % (L.tc_last_error().decode(), code.value))
+    m, z = M.value, nnz.value
+    rt = C.CDLL("libcudart.so.12")
+    rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    out = []
+    for ptr, n, dt in zip(ptrs, (m + 1, z, z), (torch.int32, torch.int32, torch.float32)):
+        t = torch.empty(n, dtype=dt, device="cuda")
+        if n:
+            assert rt.cudaMemcpy(t.data_ptr(), ptr.value, 4 * n, 3) == 0     # device to device
+        out.append(t)
+        L.tc_device_free(ptr)
+    return (m, N.value) + tuple(out), (pm.value, bm.value)
 
 
 def read_mtx(path):

@@ -194,6 +194,9 @@ tc_status tc_plan_info_get(const tc_plan *p, tc_plan_info *i)
     i->spmv_bytes = p->spmv_bytes();
     i->partition_ms = p->partition_ms;
     i->num_contours = (int)(p->corners.size() / 4);
+    i->nwtiles = p->nwtiles;
+    i->window_lo = p->wlo;
+    i->window_hi = p->whi;
     return TC_OK;
 }
 

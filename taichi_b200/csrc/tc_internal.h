@@ -55,7 +55,8 @@ enum TileKind : int {
     TILE_STREAM = 8,   // entry-parallel gather, then row-parallel sums in shared memory
     TILE_STREAM4 = 9,  // the same with 4 consecutive rows per thread (row0 % 4 == 0)
     TILE_DIRECT4 = 10,    // 4 consecutive rows per thread straight from global memory
-    TILE_DIRECT_WIDE = 11 // the same over up to 4096 rows (a 1024-thread CTA)
+    TILE_DIRECT_WIDE = 11, // the same over up to 4096 rows (a 1024-thread CTA)
+    TILE_WINDOW = 12      // rows summed from a staged x window (the window kernel's tiles)
 };
 
 struct Tile {          // 16 bytes, read once per CTA
@@ -89,6 +90,19 @@ constexpr int kDirectRows = 1024;     // most rows of a direct tile (TILE_DIRECT
 constexpr int kDirectWideBlock = 1024; // threads of the direct kernel's CTAs
 constexpr int kDirectWideRows = 4 * kDirectWideBlock;   // most rows of a TILE_DIRECT_WIDE tile
 
+// Window plans (tc_window.cu): tiles of consecutive rows whose row pointers,
+// CSR words and x window are staged in shared memory by bulk copies.
+constexpr int kWinBlock = 512;        // threads of the window kernel's CTAs (one per SM)
+constexpr int kWinRows = 1024;        // most rows of a window tile
+constexpr int kWinNnz = 8192;         // most CSR words of a window tile
+constexpr int kWinHalo = 4096;        // farthest column - row a window reaches, each side
+constexpr int kWinMaxStages = 4;      // pipeline depth (stages of one CTA)
+constexpr int kWinSmemBudget = 200 * 1024;   // shared memory of the stages
+constexpr int kWinMinRows = 1 << 16;  // smaller matrices keep the one-CTA-per-tile kernels
+constexpr double kWinCover = 0.95;    // share of the in-halo accesses the window range holds
+constexpr double kWinMinShare = 0.5;  // share of all accesses it must hold for a window plan
+constexpr double kWinMinAccesses = 2.0;   // terms per row below which the direct kernels win
+
 // Everything a multiply kernel needs about one plan (passed by value).
 struct DevPlan {
     const int *rowptr;      // M+1
@@ -107,6 +121,12 @@ struct DevPlan {
                             // every tile is a wide direct tile (the direct kernel), or 4
                             // when every tile is a stream tile (the stream kernel)
     int *err;               // device error word (1: a bounded wait gave up)
+    // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
+    const Tile *wtiles;
+    int nwtiles;
+    int wlo, whi;           // x window of rows [r0, r0 + n): [r0 + wlo, r0 + n + whi)
+    int w_rp, w_cw, w_xw;   // ints per stage: row pointers, CSR words, x window
+    int w_stages, w_grid;   // pipeline depth, persistent grid
 };
 
 struct tc_plan_impl;
@@ -136,6 +156,9 @@ struct tc_plan {
     int max_span = 0;
     int stage_rp = 8, stage_cw = 8, grid = 1;
     int *d_err = nullptr;
+    // window plan (tc_window.cu); nwtiles == 0 when the plan has none
+    tc::Tile *d_wtiles = nullptr;
+    int nwtiles = 0, wlo = 0, whi = 0, w_rp = 0, w_cw = 0, w_xw = 0, w_stages = 0, w_grid = 0;
     // host copies of the small format arrays (always) and optionally the CSR
     std::vector<int> h_xStart, h_yStart, h_xStop, h_nDiasPtr, h_offsets;
     std::vector<int> h_rowptr, h_cols;   // only with TC_FLAG_KEEP_HOST
@@ -177,6 +200,13 @@ constexpr int kStreamManyMinBlocks = 8;
 constexpr int kItemMinBlocks = 5;
 // Launch of the multiply kernel for one plan.
 tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
+// Window plans (tc_window.cu): the planner (false when the matrix does not
+// qualify), the kernels' shared-memory setup and the launch.
+bool plan_window(const tc_plan *p, const int *rowptr, const int *cols, std::vector<Tile> &wtiles, int *wlo,
+                 int *whi, int *max_rows, int *max_nnz);
+size_t window_smem_bytes(const DevPlan &dp);
+tc_status window_prepare(DevPlan &dp);
+tc_status launch_window(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
 tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,
                       cudaStream_t s);
 
@@ -198,6 +228,21 @@ struct PartitionOut {
 tc_status gpu_partition(int M, int N, int64_t nnz, const int *d_rowptr, const int *d_col,
                         const float *d_val, const tc_params &prm, bool keep_stages,
                         bool want_claimed, cudaStream_t s, PartitionOut &out);
+
+// Matrix Market entries in file order (1-based indices, checked against the
+// size line; symmetric / hermitian files flagged, not yet mirrored).
+struct MtxEntry {
+    int i, j;
+    float v;
+};
+struct MtxCoo {
+    int M = 0, N = 0;
+    bool symmetric = false;
+    std::vector<MtxEntry> entries;
+};
+// Parses a Matrix Market coordinate file (readMtx's grammar); *ref_code gets
+// the reference's code (0, -1 open, -2 banner, -3 complex, -4 size, -5 entry).
+tc_status mtx_parse(const char *path, MtxCoo &out, int *ref_code);
 
 // Dense-diagonal extraction of one shape box on host arrays (marks h_val).
 struct OneShape {

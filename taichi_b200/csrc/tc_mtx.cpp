@@ -25,10 +25,7 @@ namespace {
 
 enum Field { F_REAL, F_INT, F_PATTERN };
 
-struct Entry {
-    int i, j;
-    float v;
-};
+using Entry = tc::MtxEntry;
 
 inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
 
@@ -76,14 +73,11 @@ bool parse_span(const char *p, const char *e, Field fld, bool one_per_line, std:
 
 }  // namespace
 
-extern "C" tc_status tc_read_mtx(const char *path, int *Mo, int *No, int64_t *nnzo, int **rowptr,
-                                 int **col, float **val, int *ref_code)
+namespace tc {
+
+tc_status mtx_parse(const char *path, MtxCoo &out, int *ref_code)
 {
-    int dummy;
-    if (!ref_code) ref_code = &dummy;
     *ref_code = 0;
-    if (!path || !Mo || !No || !nnzo || !rowptr || !col || !val)
-        return tc::fail(TC_ERR_INVALID, "tc_read_mtx: null argument");
     FILE *f = fopen(path, "r");
     if (!f) { *ref_code = -1; return tc::fail(TC_ERR_IO, "cannot open %s", path); }
     char line[1025];
@@ -156,7 +150,8 @@ extern "C" tc_status tc_read_mtx(const char *path, int *Mo, int *No, int64_t *nn
             });
         for (auto &x : th) x.join();
     }
-    std::vector<Entry> all;
+    std::vector<MtxEntry> &all = out.entries;
+    all.clear();
     bool par_ok = std::all_of(part_ok.begin(), part_ok.end(), [](char c) { return c != 0; });
     if (par_ok) {
         size_t tot = 0;
@@ -175,18 +170,38 @@ extern "C" tc_status tc_read_mtx(const char *path, int *Mo, int *No, int64_t *nn
         return tc::fail(TC_ERR_IO, "%s: %zu entries, size line says %lu", path, all.size(), nz);
     }
     all.resize(nz);   // like the reference, read exactly nz entries
-
-    std::vector<int64_t> cnt((size_t)M + 1, 0);
     for (auto &en : all) {
-        if (en.i < 1 || en.i > M || en.j < 1 || en.j > N) {
+        if (en.i < 1 || en.i > M || en.j < 1 || en.j > N || (sym && en.i != en.j && en.j > M)) {
             *ref_code = -5;
             return tc::fail(TC_ERR_IO, "%s: entry (%d,%d) outside %d x %d", path, en.i, en.j, M, N);
         }
+    }
+    out.M = M;
+    out.N = N;
+    out.symmetric = sym;
+    return TC_OK;
+}
+
+}  // namespace tc
+
+extern "C" tc_status tc_read_mtx(const char *path, int *Mo, int *No, int64_t *nnzo, int **rowptr,
+                                 int **col, float **val, int *ref_code)
+{
+    int dummy;
+    if (!ref_code) ref_code = &dummy;
+    *ref_code = 0;
+    if (!path || !Mo || !No || !nnzo || !rowptr || !col || !val)
+        return tc::fail(TC_ERR_INVALID, "tc_read_mtx: null argument");
+    tc::MtxCoo coo;
+    TC_CHECK(tc::mtx_parse(path, coo, ref_code));
+    const int M = coo.M, N = coo.N;
+    const bool sym = coo.symmetric;
+    const std::vector<tc::MtxEntry> &all = coo.entries;
+
+    std::vector<int64_t> cnt((size_t)M + 1, 0);
+    for (auto &en : all) {
         cnt[en.i - 1]++;
-        if (sym && en.i != en.j) {
-            if (en.j > M) { *ref_code = -5; return tc::fail(TC_ERR_IO, "%s: symmetric entry outside", path); }
-            cnt[en.j - 1]++;
-        }
+        if (sym && en.i != en.j) cnt[en.j - 1]++;
     }
     int64_t run = 0;
     int *rp = (int *)malloc(sizeof(int) * ((size_t)M + 1));

@@ -426,6 +426,7 @@ struct Border {
     int parent;     // hole: start pixel of the enclosing outer border
     int len;        // points of the traced contour
     int mid;        // pixel index of point len/2
+    long long area2;   // twice the signed area of the contour polygon (shoelace sum)
 };
 
 __global__ void nonzero01(const int *__restrict__ f, int *__restrict__ o, int n)
@@ -446,6 +447,7 @@ __global__ void border_compact(const int *flags, const int *order, const int *pa
     b.parent = b.hole ? parent_pix[i] : -1;
     b.len = 0;
     b.mid = i;
+    b.area2 = 0;
     out[order[i]] = b;
 }
 
@@ -455,7 +457,10 @@ __constant__ int c_dy[8] = {0, -1, -1, -1, 0, 1, 1, 1};
 
 // Follows one border (Suzuki & Abe steps 3.1-3.5).  With want < 0 returns the
 // number of points; otherwise returns the pixel index of point `want`.
-__device__ long follow(const Img &img, int sy, int sx, int hole, long want, long cap, int *flag)
+// area2 (optional, with want < 0): the shoelace sum over the closed polygon
+// of the points, sum of x_i y_{i+1} - x_{i+1} y_i (twice the signed area).
+__device__ long follow(const Img &img, int sy, int sx, int hole, long want, long cap, int *flag,
+                       long long *area2 = nullptr)
 {
     const int W = img.W;
     int s = hole ? 0 : 4;
@@ -478,6 +483,7 @@ __device__ long follow(const Img &img, int sy, int sx, int hole, long want, long
             if (img.pix(ny, nx)) break;
         }
         s = k & 7;
+        if (area2) *area2 += (long long)cx * ny - (long long)nx * cy;
         if (ny == sy && nx == sx && cy == ly && cx == lx) return want < 0 ? n + 1 : -1;
         cy = ny;
         cx = nx;
@@ -494,8 +500,10 @@ __global__ void trace_kernel(Img img, Border *bs, int nb, int *flag)
     Border b = bs[i];
     const int y = b.start / img.W, x = b.start % img.W;
     const long cap = 8L * img.H * img.W + 16;
-    const long len = follow(img, y, x, b.hole, -1, cap, flag);
+    long long a2 = 0;
+    const long len = follow(img, y, x, b.hole, -1, cap, flag, &a2);
     b.len = (int)len;
+    b.area2 = a2;
     const long m = follow(img, y, x, b.hole, len / 2, cap, flag);
     b.mid = m < 0 ? b.start : (int)m;
     bs[i] = b;
@@ -725,6 +733,7 @@ void shape_size(int M, int N, int mF, int x1, int y1, int a1, int b1, int &x, in
 // ======================================================================
 struct ContourList {
     std::vector<int> lens, first, mid;   // pixel indices y*W+x
+    std::vector<long long> area2;        // twice the polygon area (signed)
 };
 
 static tc_status contours_on_device(const Img &img, cudaStream_t s, ContourList &out)
@@ -785,13 +794,15 @@ static tc_status contours_on_device(const Img &img, cudaStream_t s, ContourList 
             head[p] = i;
         }
     }
-    out.lens.clear(); out.first.clear(); out.mid.clear();
+    out.lens.clear(); out.first.clear(); out.mid.clear(); out.area2.clear();
+    auto put = [&](const Border &b) {
+        out.lens.push_back(b.len); out.first.push_back(b.start); out.mid.push_back(b.mid);
+        out.area2.push_back(b.area2);
+    };
     for (int i = nb - 1; i >= 0; --i) {
         if (hb[i].hole) continue;
-        out.lens.push_back(hb[i].len); out.first.push_back(hb[i].start); out.mid.push_back(hb[i].mid);
-        for (int j = head[i]; j >= 0; j = next[j]) {
-            out.lens.push_back(hb[j].len); out.first.push_back(hb[j].start); out.mid.push_back(hb[j].mid);
-        }
+        put(hb[i]);
+        for (int j = head[i]; j >= 0; j = next[j]) put(hb[j]);
     }
     return TC_OK;
 }
@@ -803,6 +814,7 @@ static tc_status contours_on_device(const Img &img, cudaStream_t s, ContourList 
 struct SdfOut {
     int mF = 0, W = 0;
     std::vector<int> corners;               // 4 per kept contour
+    std::vector<double> widths;             // per kept contour: area / corner distance
     std::vector<unsigned char> stages;      // 5*H*W when requested
     int ncontours = 0;                      // all contours before the length filter
 };
@@ -855,6 +867,10 @@ static tc_status getsdf_device(int M, int N, const int *d_rowptr, const int *d_c
         out.corners.push_back(cl.first[i] / W);             // contour[0].y (row)
         out.corners.push_back(cl.mid[i] % W);               // contour[size/2]
         out.corners.push_back(cl.mid[i] / W);
+        // morohutils.cu:268-272: contourArea(contour) / |contour[0] - contour[size/2]|
+        const double dx = cl.first[i] % W - cl.mid[i] % W, dy = cl.first[i] / W - cl.mid[i] / W;
+        const double area = 0.5 * std::fabs((double)cl.area2[i]);
+        out.widths.push_back(area / std::sqrt(dx * dx + dy * dy));
     }
     if (keep_stages) {
         DevBuf bytes;
@@ -1316,4 +1332,55 @@ extern "C" tc_status tc_thumbnail_noalloc(int M, int N, const int *d_rowptr, con
     if (hflag) return tc::fail(TC_ERR_UNSUPPORTED, "hole fill did not converge");
     *W_out = W;
     return TC_OK;
+}
+
+// ======================================================================
+// getSdf with the reference's C++ signature (morphutils.h:40-41)
+// ======================================================================
+#include "morphutils.h"
+
+void getSdf(std::string path, int M, int N, int nnz, int *&csrRowIndexHostPtr, int *&csrColIndexHostPtr,
+            float *&csrValHostPtr, std::string &category, Point_t &size, int &shapeNum,
+            std::vector<Point_t> &shapePoints, std::vector<double> &widths)
+{
+    (void)path;
+    (void)csrValHostPtr;
+    category = "diagonal";                        // morohutils.cu:186
+    tc_params prm;
+    tc_params_default(&prm);
+    if (M <= prm.thumb_height) {                  // morohutils.cu:192-196
+        printf("the matrix is too small! exit\n");
+        return;
+    }
+    shapeNum = 0;
+    auto report = [](tc_status st) {
+        if (st != TC_OK) printf("getSdf: %s\n", tc_last_error());
+    };
+    if (M < 0 || N < 0 || nnz < 0 || !csrRowIndexHostPtr || (nnz > 0 && !csrColIndexHostPtr)) {
+        report(tc::fail(TC_ERR_INVALID, "bad arguments"));
+        return;
+    }
+    tc::DevBuf drp, dcol;
+    tc_status st = drp.alloc(sizeof(int) * ((size_t)M + 1));
+    if (st == TC_OK) st = dcol.alloc(sizeof(int) * (size_t)std::max(nnz, 1));
+    if (st == TC_OK && cudaMemcpy(drp.p, csrRowIndexHostPtr, sizeof(int) * ((size_t)M + 1),
+                                  cudaMemcpyHostToDevice) != cudaSuccess)
+        st = tc::fail(TC_ERR_CUDA, "row pointer upload");
+    if (st == TC_OK && nnz > 0 &&
+        cudaMemcpy(dcol.p, csrColIndexHostPtr, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice) != cudaSuccess)
+        st = tc::fail(TC_ERR_CUDA, "column upload");
+    tc::SdfOut o;
+    if (st == TC_OK) st = tc::getsdf_device(M, N, drp.as<int>(), dcol.as<int>(), prm, false, nullptr, o);
+    if (st != TC_OK) {
+        report(st);
+        return;
+    }
+    size.x = o.mF;                                // morohutils.cu:262-263
+    size.y = o.W;
+    shapeNum = (int)o.corners.size() / 4;
+    for (int i = 0; i < shapeNum; ++i) {
+        shapePoints.push_back(Point_t{o.corners[4 * i], o.corners[4 * i + 1]});
+        shapePoints.push_back(Point_t{o.corners[4 * i + 2], o.corners[4 * i + 3]});
+        widths.push_back(o.widths[i]);
+    }
 }

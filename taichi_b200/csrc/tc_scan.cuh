@@ -1,6 +1,8 @@
 // tc_scan.cuh -- device-wide exclusive prefix sum of int32 (used by the
-// partitioner's compactions).  Two-level reduce-then-scan with 4096 elements
-// per 256-thread block; recursion on the block totals.
+// partitioner's compactions and the device format build).  Two-level
+// reduce-then-scan with 4096 elements per 256-thread block; recursion on the
+// block totals.  The kernels have internal linkage: each file that includes
+// this header gets its own copies.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -9,6 +11,7 @@
 
 namespace tc {
 namespace scan_detail {
+namespace {
 
 constexpr int kThreads = 256;
 constexpr int kItems = 16;
@@ -72,11 +75,12 @@ __global__ void add_offsets(int *__restrict__ out, int n, const int *__restrict_
     for (int i = threadIdx.x; i < kTile && base + i < n; i += kThreads) out[base + i] += add;
 }
 
+}  // namespace
 }  // namespace scan_detail
 
 // Exclusive scan of n ints; writes n+1 values (out[n] = total).  `tmp` must
 // hold scan_tmp_ints(n) ints.  in and out may alias.
-inline size_t scan_tmp_ints(long n)
+static inline size_t scan_tmp_ints(long n)
 {
     size_t t = 0;
     long m = n + 1;
@@ -87,7 +91,7 @@ inline size_t scan_tmp_ints(long n)
     return t + 2;
 }
 
-inline tc_status exclusive_scan(const int *in, int *out, long n, int *tmp, cudaStream_t s)
+static inline tc_status exclusive_scan(const int *in, int *out, long n, int *tmp, cudaStream_t s)
 {
     using namespace scan_detail;
     // treat the input as n+1 values with a trailing 0 so out[n] is the total

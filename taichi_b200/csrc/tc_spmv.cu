@@ -19,6 +19,7 @@
 
 #include "tc_internal.h"
 #include "tc_tile.cuh"
+#include "tc_tma.cuh"
 
 namespace tc {
 
@@ -128,82 +129,6 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, int min_tiles, std::
 
 // ------------------------------------------------------------------ kernels
 namespace {
-
-// ---- TMA bulk copies into shared memory, completion on an mbarrier ----
-__device__ __forceinline__ unsigned smem_u32(const void *p)
-{
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *m, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)),
-                 "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *m)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m)) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t *m, unsigned parity)
-{
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_u32(m)), "r"(parity) : "memory");
-    return ok != 0;
-}
-// Nanoseconds of the GPU's global timer.
-__device__ __forceinline__ uint64_t globaltimer_ns()
-{
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Bounded wait: gives up once kStageWaitNs of global-timer time have passed
-// since the first failed poll (the copies complete in microseconds; a
-// give-up is reported through the plan's error word).  The deadline is time,
-// not a poll count, because each try_wait may suspend the thread for a
-// hardware-chosen interval.
-constexpr uint64_t kStageWaitNs = 1000000000ull;   // 1 s
-
-__device__ __forceinline__ bool mbar_wait(uint64_t *m, unsigned parity)
-{
-    if (mbar_test(m, parity)) return true;
-    const uint64_t t0 = globaltimer_ns();
-    for (;;) {
-        for (int i = 0; i < 32; ++i)
-            if (mbar_test(m, parity)) return true;
-        if (globaltimer_ns() - t0 > kStageWaitNs) return false;
-    }
-}
-__device__ __forceinline__ void fence_async_shared()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// 16-byte aligned byte window [a, b) that covers elements [e0, e1) of an
-// int array (the plan arrays are padded, so the window stays inside them).
-struct Window {
-    long a, b;
-    int shift;   // index of element e0 inside the window
-};
-__device__ __forceinline__ Window window_of(long e0, long e1)
-{
-    Window w;
-    w.a = (e0 * 4) & ~15L;
-    w.b = (e1 * 4 + 15) & ~15L;
-    w.shift = (int)((e0 * 4 - w.a) >> 2);
-    return w;
-}
 
 // Issues the copies of tile t into stage s (thread 0 only).
 __device__ __forceinline__ void stage_tile(const DevPlan &p, int t, int *rp_buf, int *cw_buf,
@@ -493,6 +418,7 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
 tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s)
 {
     if (dp.M == 0) return TC_OK;
+    if (dp.nwtiles > 0) return launch_window(dp, x, y, s);
     return dp.hybrid ? launch_tiles<true>(dp, x, y, s) : launch_tiles<false>(dp, x, y, s);
 }
 
@@ -543,6 +469,15 @@ tc::DevPlan tc_plan::dev_plan() const
                : ntiles_stream == ntiles ? 4
                : ntiles_lanes == 0 ? 2 : 1;
     d.err = d_err;
+    d.wtiles = d_wtiles;
+    d.nwtiles = nwtiles;
+    d.wlo = wlo;
+    d.whi = whi;
+    d.w_rp = w_rp;
+    d.w_cw = w_cw;
+    d.w_xw = w_xw;
+    d.w_stages = w_stages;
+    d.w_grid = w_grid;
     return d;
 }
 
@@ -629,6 +564,33 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     }
     for (Tile &t : tiles) t.nrows_kind |= diag_class(p, t.row0, t.row0 + tile_nrows(t)) << kDiagShift;
 
+    // window plan: a second tile list for the window kernel (the batch and
+    // served launches keep running `tiles`, with the same terms and order)
+    std::vector<Tile> wtiles;
+    p->nwtiles = 0;
+    {
+        int wlo = 0, whi = 0, wrows = 0, wnnz = 0;
+        if (plan_window(p, csrRow, csrCol, wtiles, &wlo, &whi, &wrows, &wnnz)) {
+            const int w_rp = (wrows + 8 + 3) & ~3, w_cw = (wnnz + 8 + 3) & ~3;
+            const int w_xw = (wrows + whi - wlo + 8 + 3) & ~3;
+            const size_t stage = 4 * (size_t)(w_rp + w_cw + w_xw);
+            const int S = (int)std::min<size_t>(kWinMaxStages, (kWinSmemBudget - 128) / stage);
+            if (S >= 2) {
+                p->nwtiles = (int)wtiles.size();
+                p->wlo = wlo;
+                p->whi = whi;
+                p->w_rp = w_rp;
+                p->w_cw = w_cw;
+                p->w_xw = w_xw;
+                p->w_stages = S;
+                p->w_grid = std::min(p->nwtiles, num_sms());
+                for (Tile &t : wtiles) t.nrows_kind |= diag_class(p, t.row0, t.row0 + tile_nrows(t)) << kDiagShift;
+            } else {
+                wtiles.clear();
+            }
+        }
+    }
+
     size_t o_rp = 0;
     size_t o_cols = align256(o_rp + sizeof(int) * ((size_t)M + 1) + 16);
     size_t o_tiles = align256(o_cols + sizeof(int) * (size_t)p->nnz_csr + 16);
@@ -636,7 +598,8 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     size_t o_sd = align256(o_sh + sizeof(int4) * shapes.size());
     size_t o_off = align256(o_sd + sizeof(int2) * sd.size());
     size_t o_err = align256(o_off + sizeof(int) * (size_t)p->num_negs + 16);
-    size_t total = align256(o_err + 16);
+    size_t o_wt = align256(o_err + 16);
+    size_t total = align256(o_wt + sizeof(Tile) * wtiles.size());
     char *base = nullptr;
     cudaError_t e = cudaMalloc(&base, total);
     if (e != cudaSuccess)
@@ -650,6 +613,7 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     p->d_shape_dias = reinterpret_cast<int2 *>(base + o_sd);
     p->d_offsets = reinterpret_cast<int *>(base + o_off);
     p->d_err = reinterpret_cast<int *>(base + o_err);
+    p->d_wtiles = p->nwtiles ? reinterpret_cast<Tile *>(base + o_wt) : nullptr;
     {   // persistent grid: CTAs per SM from occupancy at this stage size
         DevPlan tmp = p->dev_plan();
         const size_t smem = stream_smem_bytes(tmp);
@@ -669,6 +633,12 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     if (!tiles.empty())
         TC_CUDA(cudaMemcpyAsync(p->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(),
                                 cudaMemcpyHostToDevice, stream));
+    if (p->nwtiles) {
+        TC_CUDA(cudaMemcpyAsync(p->d_wtiles, wtiles.data(), sizeof(Tile) * wtiles.size(),
+                                cudaMemcpyHostToDevice, stream));
+        DevPlan dp = p->dev_plan();
+        TC_CHECK(window_prepare(dp));
+    }
     if (!shapes.empty()) {
         TC_CUDA(cudaMemcpyAsync(p->d_shapes, shapes.data(), sizeof(int4) * shapes.size(),
                                 cudaMemcpyHostToDevice, stream));

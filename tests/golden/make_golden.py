@@ -12,6 +12,8 @@
 
 Needs cv2 and oracle/_ref, i.e. a machine with the reference checkout.
 Run from the repository root:  python tests/golden/make_golden.py
+(``--widths`` writes only sdf_widths.json, getSdf's per-contour widths,
+which needs cv2 alone.)
 """
 import hashlib
 import json
@@ -88,7 +90,28 @@ def cv2_getsdf(M, N, rowptr, col):
     cs = [c for c in cv2_contours(eo) if len(c) >= 80]
     corners = np.array([[c[0][0], c[0][1], c[len(c) // 2][0], c[len(c) // 2][1]] for c in cs],
                        np.int32).reshape(-1, 4)
+    cv2_getsdf.widths = [cv2_width(c) for c in cs]
     return 512, W, corners, [rev, filled, o2, dele, eo]
+
+
+def cv2_width(c):
+    """morohutils.cu:268-272: contourArea(contour) / |contour[0] - contour[size/2]|."""
+    a, b = c[0].astype(np.float64), c[len(c) // 2].astype(np.float64)
+    d = np.sqrt((a[0] - b[0]) ** 2 + (a[1] - b[1]) ** 2)
+    area = cv2.contourArea(c.reshape(-1, 1, 2))
+    return float(area / d) if d > 0 else float("inf")
+
+
+def sdf_widths():
+    """getSdf's widths output (area / corner distance per kept contour) for
+    every matrix case, written to sdf_widths.json."""
+    out = {}
+    for c in cases.MATRIX_CASES:
+        M, N, rp, col = cases.matrix(c)
+        cv2_getsdf.widths = []
+        cv2_getsdf(M, N, rp, col)
+        out[c["name"]] = cv2_getsdf.widths
+    return out
 
 
 def images():
@@ -164,6 +187,11 @@ def mtx():
 
 
 def main():
+    if "--widths" in sys.argv:          # sdf_widths.json only
+        with open(os.path.join(HERE, "sdf_widths.json"), "w") as f:
+            json.dump(dict(_doc="cv2 4.13.0 getSdf widths (morohutils.cu:268-272) per matrix case, "
+                                "made by make_golden.py --widths", widths=sdf_widths()), f, indent=1)
+        return
     obuild.build_oracle()
     if obuild.build_ref() is None:
         sys.exit("set TAICHI_REFERENCE to the reference checkout to build oracle/_ref")

@@ -18,7 +18,8 @@ def header_c_symbols():
 
 def header_cpp_symbols():
     text = open(os.path.join(ROOT, "include", "TaiChi.h")).read()
-    return sorted(set(re.findall(r"TAICHI_API\s+\w+\s+(\w+)\s*\(", text)))
+    text += open(os.path.join(ROOT, "include", "morphutils.h")).read()
+    return sorted(set(re.findall(r"TAICHI(?:_MORPH)?_API\s+\w+\s+(\w+)\s*\(", text)))
 
 
 def test_c_symbols_exported(tc):
@@ -40,7 +41,12 @@ def test_cpp_compat_symbols_exported(tc):
     for sig in ("readMtx(char*, int&, int&, unsigned long&, int*&, int*&, float*&)",
                 "partition_shapes(char*, int, int, int, int*&, int*&, float*&, TaiChi_new*)",
                 "taichi_SpMV(int, int, TaiChi_new*, float*, float*)",
-                "free_taichi_new(TaiChi_new*)"):
+                "free_taichi_new(TaiChi_new*)",
+                "getSdf(std::__cxx11::basic_string<char, std::char_traits<char>, std::allocator<char> >, "
+                "int, int, int, int*&, int*&, float*&, std::__cxx11::basic_string<char, "
+                "std::char_traits<char>, std::allocator<char> >&, Point_t&, int&, "
+                "std::vector<Point_t, std::allocator<Point_t> >&, std::vector<double, "
+                "std::allocator<double> >&)"):
         assert sig in out, sig
 
 

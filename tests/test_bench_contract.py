@@ -38,20 +38,27 @@ def test_reference_arm_other_ranks_idle():
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
 
 
-def test_refine_rate_bisection():
-    """The served form's rate search: a fake server whose p99 grows with the
-    rate (2 ms at 2,000 requests/s) and which serves every rate in full."""
+def test_highest_passing_rate():
+    """The served form's rate search against a fake server whose p99 grows
+    with the rate (2 ms at 2,000 requests/s) and which serves every rate in
+    full: the sweep stops at the first failing rate and the bisection closes
+    in on 2,000 from below."""
     sys.path.insert(0, ROOT)
     import bench
     calls = []
 
-    def p99_at(rate):
+    def serve_at(rate):
         calls.append(rate)
-        return rate / 1000.0, rate
+        return {"p99_ms": rate / 1000.0, "spmv_per_s": rate}
 
-    rate, tput = bench.refine_rate(p99_at, (1000.0, 1000.0), 4000.0, 6)
-    assert len(calls) == 6
-    assert 2000.0 - 3000.0 / 64 <= rate < 2000.0 and tput == rate
-    # nothing passes above the start: the start is kept
-    rate, tput = bench.refine_rate(lambda r: (5.0, r), (1000.0, 900.0), 4000.0, 3)
-    assert (rate, tput) == (1000.0, 900.0)
+    best, runs = bench.highest_passing_rate(serve_at, [500.0, 1000.0, 4000.0, 8000.0], 6)
+    assert calls[:3] == [500.0, 1000.0, 4000.0] and len(calls) == 3 + 6
+    assert 2000.0 - 3000.0 / 64 <= best["spmv_per_s"] < 2000.0
+    assert len(runs) == len(calls)
+    # nothing passes: no best run, and no bisection
+    calls.clear()
+    best, runs = bench.highest_passing_rate(lambda r: {"p99_ms": 5.0, "spmv_per_s": r}, [100.0, 200.0], 4)
+    assert best is None and len(runs) == 1
+    # everything passes: the highest rate, no bisection
+    best, runs = bench.highest_passing_rate(lambda r: {"p99_ms": 0.1, "spmv_per_s": r}, [1.0, 2.0, 3.0], 4)
+    assert best["spmv_per_s"] == 3.0 and len(runs) == 3

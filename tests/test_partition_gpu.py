@@ -158,6 +158,18 @@ def test_compat_readmtx_partition_spmv(tc, dev, golden, tmp_path, monkeypatch):
     y = np.zeros(M, np.float32)
     spmv(M, N, t, x.ctypes.data_as(C.POINTER(C.c_float)), y.ctypes.data_as(C.POINTER(C.c_float)))
     np.testing.assert_array_equal(y, np.diff(rp).astype(np.float32))   # main.cu:61-86 check
+    # beyond the reference's own x = 1 check: integer x (exact) and FP32 x
+    # (normwise within 1e-5 of the FP64 oracle)
+    rng = np.random.default_rng(13)
+    xi = rng.integers(-8, 9, N).astype(np.float32)
+    spmv(M, N, t, xi.ctypes.data_as(C.POINTER(C.c_float)), y.ctypes.data_as(C.POINTER(C.c_float)))
+    np.testing.assert_array_equal(y.astype(np.float64), oracle.spmv_csr_f64(M, rp, col, xi.astype(np.float64)))
+    xf = rng.uniform(-1, 1, N).astype(np.float32)
+    spmv(M, N, t, xf.ctypes.data_as(C.POINTER(C.c_float)), y.ctypes.data_as(C.POINTER(C.c_float)))
+    y64 = oracle.spmv_csr_f64(M, rp, col, xf.astype(np.float64))
+    rel = np.linalg.norm(y.astype(np.float64) - y64) / np.linalg.norm(y64)
+    print("taichi_SpMV FP32 x: normwise rel err %.2e" % rel)
+    assert rel <= 1e-5
     _cpp(tc, "_Z15free_taichi_newP10TaiChi_new")(t)
     for p in (prp, pcol, pval):
         libc.free(C.cast(p, C.c_void_p))

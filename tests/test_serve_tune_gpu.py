@@ -107,3 +107,102 @@ def test_tuner(tc, dev):
     print("tuned: density %.2f tile_rows %d max_lanes %d ctas/SM %d: %.2f us (default %.2f us)" % (
         r.params.density, r.params.tile_rows, r.params.max_lanes, r.params.ctas_per_sm, r.spmv_us,
         r.default_us))
+
+
+def test_online_submit_poll_wait(tc, dev):
+    """The online interface: requests submitted from two threads while the
+    dispatcher batches them, completed through poll and wait; every y equals
+    the matrix's solo multiply bit for bit.  Then the host-vector form."""
+    import threading
+    import torch
+    plans, mats = make_plans(tc)
+    srv = tc.Server(contexts=3, max_batch=32, max_inflight=2, arena_bytes=64 << 20)
+    ids = [srv.admit(p) for p in plans]
+    rng = np.random.default_rng(21)
+    n = 400
+    matrix = rng.integers(0, len(plans), n)
+    xs = [torch.from_numpy(rng.uniform(-1, 1, mats[m][1]).astype(np.float32)) for m in matrix]
+    want = [solo(plans[m], x.numpy(), mats[m][0], dev) for m, x in zip(matrix, xs)]
+    for device_vectors in (True, False):
+        if device_vectors:
+            X = [x.to(dev) for x in xs]
+            Y = [torch.full((mats[m][0],), float("nan"), device=dev) for m in matrix]
+        else:
+            X = [x.pin_memory() for x in xs]
+            Y = [torch.full((mats[m][0],), float("nan")).pin_memory() for m in matrix]
+        srv.start(device_vectors=device_vectors)
+        tickets = [None] * n
+
+        def feed(lo):
+            for r in range(lo, n, 2):
+                tickets[r] = srv.submit(ids[matrix[r]], X[r], Y[r])
+
+        th = [threading.Thread(target=feed, args=(k,)) for k in (0, 1)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        import time
+        pending, t0 = set(range(n)), time.time()
+        while pending:                       # poll until all are done
+            pending = {r for r in pending if not srv.poll(tickets[r])}
+            assert time.time() - t0 < 60, "%d requests not done after 60 s" % len(pending)
+        srv.wait(tickets[-1], 10.0)
+        st = srv.stats()
+        srv.stop()
+        assert st["requests"] == n and st["batches"] >= 1
+        for r in range(n):
+            np.testing.assert_array_equal(Y[r].cpu().numpy(), want[r], err_msg="request %d" % r)
+        print("online %s: %d batches, mean batch %.1f, p99 %.3f ms" % (
+            "device" if device_vectors else "host", st["batches"], st["mean_batch"], st["p99_ms"]))
+    with pytest.raises(tc.TcError):
+        srv.submit(ids[0], X[0], Y[0])          # stopped
+    srv.close()
+
+
+def test_served_pool_48(tc, dev):
+    """The served workload's own pool (48 resident matrices: R-MAT scales
+    14-22 and banded matrices of 1e4-4e6 rows), 1,500 requests with Zipf(1.1)
+    matrix choice arriving as a Poisson stream: each y bit-identical to the
+    matrix's solo multiply of the same x (alone vs in the mix), and within
+    1e-5 of the FP64 oracle normwise on every request of a strided sample."""
+    import torch
+    from taichi_b200 import workloads
+    mats = workloads.pool_matrices("serve", 48, 11)
+    srv = tc.Server(contexts=4, max_batch=64, max_inflight=2, arena_bytes=256 << 20)
+    plans, ids = [], []
+    for name, M, rp, col in mats:
+        p = tc.Plan.from_csr(M, M, rp, col)
+        plans.append(p)
+        ids.append(srv.admit(p))
+    rng = np.random.default_rng(31)
+    pz = np.arange(1, 49, dtype=np.float64) ** -1.1
+    pz /= pz.sum()
+    n = 1500
+    matrix = rng.choice(48, size=n, p=pz)
+    xs = [torch.empty(m[1], device=dev).uniform_(-1, 1) for m in mats]      # one x per matrix
+    solo_y = []
+    for p, x, m in zip(plans, xs, mats):
+        y = torch.empty(m[1], device=dev)
+        p.spmv(x, y)
+        solo_y.append(y)
+    ys = [torch.full((mats[m][1],), float("nan"), device=dev) for m in matrix]
+    arrival = np.cumsum(rng.exponential(1.0 / 50000, n))
+    stats, lat = srv.run(arrival, [ids[m] for m in matrix], [xs[m] for m in matrix], ys,
+                         mode=tc.SERVE_DEVICE_VECTORS)
+    torch.cuda.synchronize()
+    assert stats["requests"] == n
+    for r in range(n):
+        assert torch.equal(ys[r], solo_y[matrix[r]]), "request %d (matrix %d)" % (r, matrix[r])
+    worst = 0.0
+    for r in range(0, n, 61):
+        name, M, rp, col = mats[matrix[r]]
+        y64 = oracle.spmv_csr_f64(M, rp, col, xs[matrix[r]].cpu().numpy().astype(np.float64))
+        rel = np.linalg.norm(ys[r].cpu().numpy() - y64) / np.linalg.norm(y64)
+        worst = max(worst, rel)
+        assert rel <= 1e-5, (r, name, rel)
+    print("pool48: %.0f SpMV/s, p50 %.3f ms, p99 %.3f ms, mean batch %.1f, worst rel err %.2e" % (
+        stats["spmv_per_s"], stats["p50_ms"], stats["p99_ms"], stats["mean_batch"], worst))
+    srv.close()
+    for p in plans:
+        p.close()

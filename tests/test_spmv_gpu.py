@@ -313,16 +313,115 @@ def test_stream_kernel_many_tiles(tc, dev):
     the plain CSR plan of the same mesh, both against the oracle."""
     import torch
     M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=9)
-    plan = tc.Plan.from_csr(M, N, rp, col)
+    no_window = tc.params(flags=tc.TC_FLAG_NO_WINDOW)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=no_window)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    assert plan.info()["ntiles"] > 6 * sms
+    assert plan.info()["ntiles"] > 6 * sms and plan.info()["nwtiles"] == 0
     check_plan(plan, plan.export(), M, N, rp, col, dev, "stream/many")
     x = np.random.default_rng(3).uniform(-1, 1, N).astype(np.float32)
     y_many = run_spmv(plan, x, M, dev)
     plan.close()
-    plan = tc.Plan.from_csr(M, N, rp, col, partition=False)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW), partition=False)
     y_plain = run_spmv(plan, x, M, dev)
     plan.close()
     y64 = oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64))
     assert np.linalg.norm(y_many - y64) <= TOL * np.linalg.norm(y64)
     assert np.linalg.norm(y_plain - y64) <= TOL * np.linalg.norm(y64)
+
+
+def test_spmv_mesh2048_full_size(tc, dev):
+    """The 9-point stencil on a 2048 x 2048 grid with 2% of its rows permuted
+    (37.7 M non-zeros, the one plain configuration larger than L2), formatted
+    by the GPU partitioner (whose format equals the reference's for this
+    matrix, see test_partition_gpu): integer x exact, x = 1, FP32 x within
+    1e-5 of FP64 normwise and per row.  The default plan is a window plan;
+    the stream-tile plan of the same format gives the same y bit for bit."""
+    case = next(c for c in cases.MATRIX_CASES if c["name"] == "mesh2048")
+    M, N, rp, col = cases.matrix(case)
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    info = plan.info()
+    assert info["dia_shapes"] == 1 and info["nwtiles"] > 0, info
+    fmt = plan.export()
+    check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/window")
+    x = np.random.default_rng(17).uniform(-1, 1, N).astype(np.float32)
+    y_win = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW))
+    assert plan.info()["nwtiles"] == 0
+    check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/stream")
+    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_win)
+    plan.close()
+
+
+WINDOW_CASES = [c for c in PARTITION_CASES if c["name"] in
+                ("band_holes", "two_segments", "offdiag_blocks", "wide_band", "overlap", "rect_cols",
+                 "multi_shape", "many_shapes", "cfg1_small", "rmat16_selfloops")]
+
+
+@pytest.mark.parametrize("rows", [1024, 100, 7])
+@pytest.mark.parametrize("case", WINDOW_CASES, ids=[c["name"] for c in WINDOW_CASES])
+def test_window_plans(tc, dev, case, rows):
+    """Window plans forced on every kind of matrix (one and many shapes,
+    shapes off the main diagonal, rectangular, random columns, short and
+    odd tile heights): against the oracle, and bit-identical to the
+    stream-tile plan of the same format when every row is short enough for
+    one-row-per-thread tiles (the same terms in the same order)."""
+    M, N, rp, col = cases.matrix(case)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(tile_rows=rows, flags=tc.TC_FLAG_WINDOW))
+    assert plan.info()["nwtiles"] >= (M + rows - 1) // rows
+    label = "%s/window%d" % (case["name"], rows)
+    check_plan(plan, fmt, M, N, rp, col, dev, label)
+    x = np.random.default_rng(5).uniform(-1, 1, N).astype(np.float32)
+    y_win = run_spmv(plan, x, M, dev)
+    plan.close()
+    if np.diff(fmt["csrRow"]).max(initial=0) <= 128:
+        plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW))
+        np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_win, err_msg=label)
+        plan.close()
+
+
+def test_window_unaligned_vectors(tc, dev):
+    """x and y that are not 16-byte aligned: the window kernel then reads
+    every term from global memory (no window copies), same y."""
+    import torch
+    M, N, rp, col = matgen.mesh9(grid=384, permute_frac=0.02, seed=4)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=tc.TC_FLAG_WINDOW))
+    assert plan.info()["nwtiles"] > 0
+    x = np.random.default_rng(8).integers(-8, 9, N).astype(np.float32)
+    xb = torch.zeros(N + 1, dtype=torch.float32, device=dev)
+    xb[1:] = to_dev(x, dev)
+    yb = torch.full((M + 1,), float("nan"), dtype=torch.float32, device=dev)
+    plan.spmv(xb[1:].data_ptr(), yb[1:].data_ptr())
+    torch.cuda.synchronize()
+    plan.check()
+    want = oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64))
+    np.testing.assert_array_equal(yb[1:].cpu().numpy().astype(np.float64), want)
+    plan.close()
+
+
+def test_window_plan_selection(tc, dev):
+    """The planner picks a window plan for a mesh and banded matrices, and
+    not for an R-MAT graph (rows averaging under one entry) or a small
+    matrix; TC_FLAG_NO_WINDOW turns it off."""
+    M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=1)
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    i = plan.info()
+    assert i["nwtiles"] > 0 and i["window_lo"] <= -2049 and i["window_hi"] >= 2049, i
+    plan.close()
+    rp, col = tc.gen_banded(300000, 4, 3, seed=2)
+    plan = tc.Plan.from_csr(300000, 300000, rp, col)
+    i = plan.info()
+    assert i["nwtiles"] > 0 and i["window_lo"] >= -64 and i["window_hi"] <= 64, i
+    plan.close()
+    plan = tc.Plan.from_csr(300000, 300000, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW))
+    assert plan.info()["nwtiles"] == 0
+    plan.close()
+    M, rp, col = tc.gen_rmat(18, 16, 0.499, 0.001, 0.001, seed=1)
+    plan = tc.Plan.from_csr(M, M, rp, col)
+    assert plan.info()["nwtiles"] == 0
+    plan.close()
+    M, N, rp, col = cases.matrix(next(c for c in cases.MATRIX_CASES if c["name"] == "band_holes"))
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    assert plan.info()["nwtiles"] == 0                      # 20,000 rows: below the window minimum
+    plan.close()
