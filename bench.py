@@ -163,7 +163,25 @@ def run_reference(args, rank):
                                        "rows split over %d OpenMP threads)" % (args.steps, threads)},
             "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if args.workload in ("rmat20", "small") and os.path.exists("/dev/nvidiactl") and not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu(args.workload)
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu(workload):
+    """Context beside the reference arm: the reference's own CUDA multiply
+    (TaiChi.cu compiled unmodified for sm_100a, oracle/_ref) on the same
+    matrix, timed by the reference itself (its printed spmv_time), in a child
+    process because taichi_SpMV ends with cudaDeviceReset."""
+    try:
+        r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu", "--workload", workload], cwd=ROOT,
+                           stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, timeout=300)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "oracle.ref_gpu did not finish in 300 s"}
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": "oracle.ref_gpu exited %d: %s" % (r.returncode, r.stderr.strip()[-300:])}
+    return json.loads(lines[-1])
 
 
 def run_ours(args, rank, world, local_rank):
@@ -622,6 +640,8 @@ def main():
                     help="served form, device vectors: arrival rates swept (requests/s)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip the reference's own GPU multiply (context record)")
     ap.add_argument("--tile-mode", type=int, default=None, help="0 merge, 1 lanes, 2 stream")
     ap.add_argument("--tile-rows", type=int, default=None, help="most rows per multiply tile")
     ap.add_argument("--rows-strided", action="store_true", help="stream tiles: one row per thread")

@@ -146,18 +146,24 @@ extern "C" tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const
         f.xStop = best_plan->h_xStop.data(); f.nDiasPtr = best_plan->h_nDiasPtr.data();
         f.neg_offsets = best_plan->h_offsets.data();
         f.csrRow = rp.data(); f.csrCol = cw.data();
-        // {tile_mode, tile_rows, max_lanes, ctas_per_sm}, most promising first
-        const int cand[][4] = {{2, 1024, 32, 4}, {2, 2048, 32, 4}, {1, 1024, 32, 4}, {0, 512, 32, 4},
-                               {2, 512, 32, 4}, {0, 2048, 32, 4}, {1, 1024, 8, 4}, {0, 1024, 32, 8},
-                               {1, 1024, 32, 2}, {0, 256, 32, 4}, {0, 512, 32, 8}, {0, 1024, 32, 2}};
+        // {tile_mode, tile_rows, max_lanes, ctas_per_sm, window flag}, most
+        // promising first (window flag: 0 the planner's choice, else forced
+        // on / off)
+        const int W = TC_FLAG_WINDOW, NW = TC_FLAG_NO_WINDOW;
+        const int cand[][5] = {{2, 1024, 32, 4, 0}, {2, 1024, 32, 4, W}, {2, 1024, 32, 4, NW},
+                               {2, 512, 32, 4, W}, {2, 2048, 32, 4, 0}, {1, 1024, 32, 4, 0},
+                               {0, 512, 32, 4, 0}, {2, 512, 32, 4, 0}, {0, 2048, 32, 4, 0},
+                               {1, 1024, 8, 4, 0}, {0, 1024, 32, 8, 0}, {1, 1024, 32, 2, 0},
+                               {0, 256, 32, 4, 0}, {0, 512, 32, 8, 0}, {0, 1024, 32, 2, 0}};
         for (const auto &cnd : cand) {
                     if (st != TC_OK || trials >= max_trials) break;
                     tc_params q = best.params;
                     q.tile_mode = cnd[0]; q.tile_rows = cnd[1]; q.max_lanes = cnd[2];
                     q.ctas_per_sm = cnd[3];
-                    q.flags &= ~TC_FLAG_KEEP_HOST;
+                    q.flags = (q.flags & ~(TC_FLAG_KEEP_HOST | W | NW)) | cnd[4];
                     if (q.tile_mode == best.params.tile_mode && q.tile_rows == best.params.tile_rows &&
-                        q.max_lanes == best.params.max_lanes && q.ctas_per_sm == best.params.ctas_per_sm)
+                        q.max_lanes == best.params.max_lanes && q.ctas_per_sm == best.params.ctas_per_sm &&
+                        (q.flags & (W | NW)) == (best.params.flags & (W | NW)))
                         continue;
                     tc_plan *p = nullptr;
                     st = tc_plan_from_format(M, N, &f, &q, stream, &p);
