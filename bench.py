@@ -208,6 +208,8 @@ def run_ours(args, rank, world, local_rank):
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_WINDOW
     if args.window:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WINDOW
+    if args.no_bounds:
+        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_BOUNDS
     if args.tile_nnz is not None:
         over["tile_nnz"] = args.tile_nnz
     if args.ctas_per_sm is not None:
@@ -564,7 +566,8 @@ def served_record(args):
     dev = torch.device("cuda", 0)
     mats = workloads.pool_matrices("serve", 48, 11)
     srv = tc.Server(contexts=args.serve_contexts, max_batch=args.serve_max_batch,
-                    max_inflight=args.serve_inflight, arena_bytes=512 << 20, hbm_budget=96 << 30)
+                    max_inflight=args.serve_inflight, arena_bytes=512 << 20, hbm_budget=96 << 30,
+                    solo_bytes=int(args.serve_solo_mb * 2 ** 20))
     plans, ids = [], []
     for name, M, rp, col in mats:
         p = tc.Plan.from_csr(M, M, rp, col)
@@ -582,10 +585,11 @@ def served_record(args):
     xd = [[x.to(dev) for x in pair] for pair in xh]
     yd = [[torch.empty(m[1], device=dev) for _ in range(nbuf[i])] for i, m in enumerate(mats)]
     nreq = args.requests
-    keys = ("spmv_per_s", "p50_ms", "p99_ms", "mean_batch")
+    keys = ("spmv_per_s", "p50_ms", "p99_ms", "mean_batch", "mean_service_ms", "mean_launch_us")
     out = {"requests": nreq, "pool": len(mats), "pool_rows": int(sum(m[1] for m in mats)),
            "contexts": args.serve_contexts, "max_batch": args.serve_max_batch,
-           "max_inflight": args.serve_inflight, "bisection_steps": args.rate_search}
+           "max_inflight": args.serve_inflight, "solo_mb": args.serve_solo_mb,
+           "bisection_steps": args.rate_search}
     clocks = Clocks(0)
     clocks.start()
     for form, bit, rates, XB, YB in (("device", tc.SERVE_DEVICE_VECTORS, args.device_rates, xd, yd),
@@ -650,9 +654,13 @@ def main():
     ap.add_argument("--no-direct", action="store_true", help="stream tiles only, no direct tiles")
     ap.add_argument("--no-window", action="store_true", help="never the window kernel")
     ap.add_argument("--window", action="store_true", help="the window kernel wherever rows fit its tiles")
+    ap.add_argument("--no-bounds", action="store_true",
+                    help="wide plans: the kernel that reads tile word ranges from the tile list")
     ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")
     ap.add_argument("--serve-max-batch", type=int, default=64, help="served form: most requests per launch")
     ap.add_argument("--serve-inflight", type=int, default=2, help="served form: batches on the GPU at once")
+    ap.add_argument("--serve-solo-mb", type=float, default=0.0,
+                    help="served form: matrices moving at least this many MB per SpMV get their own launch")
     ap.add_argument("--rate-search", type=int, default=4,
                     help="served form: bisection steps between the last passing and first failing rate")
     args = ap.parse_args()

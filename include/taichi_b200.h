@@ -78,6 +78,9 @@ typedef struct tc_params {
 #define TC_FLAG_NO_WINDOW    0x40 /* tile_mode 2: never run the window kernel
                                      (x staged in shared memory per tile of
                                      rows), even for a banded matrix        */
+#define TC_FLAG_NO_BOUNDS    0x100 /* wide plans: the kernel that reads each
+                                     tile's word range from the tile list
+                                     (not from the launch parameters)       */
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */
@@ -319,6 +322,10 @@ typedef struct tc_serve_config {
                              batch launches when fewer are in flight, with every
                              request waiting by then                            */
     int max_pending;      /* online requests outstanding at once (65536)         */
+    int64_t solo_bytes;   /* a request whose matrix moves at least this many
+                             bytes per SpMV runs its own multiply launch (the
+                             kernel tc_spmv picks) inside its batch instead of
+                             sharing the batch's launch (0: never, the default) */
 } tc_serve_config;
 
 typedef struct tc_serve_stats {
@@ -327,6 +334,8 @@ typedef struct tc_serve_stats {
     double spmv_per_s;    /* requests / seconds                                  */
     double p50_ms, p99_ms, mean_ms, max_ms;   /* completion - arrival            */
     double mean_batch;    /* requests per launch                                 */
+    double mean_service_ms;   /* batch launch to its completion seen (batching)  */
+    double mean_launch_us;    /* host time to pack and launch one batch          */
 } tc_serve_stats;
 
 TC_API void tc_serve_config_default(tc_serve_config *c);

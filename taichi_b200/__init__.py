@@ -24,6 +24,7 @@ TC_FLAG_NO_DIRECT = 0x10
 TC_FLAG_NO_WIDE = 0x20
 TC_FLAG_NO_WINDOW = 0x40
 TC_FLAG_WINDOW = 0x80
+TC_FLAG_NO_BOUNDS = 0x100
 
 _IP = C.POINTER(C.c_int)
 
@@ -192,13 +193,14 @@ def _stream(s):
 class ServeConfig(C.Structure):
     _fields_ = [("hbm_budget", C.c_int64), ("arena_bytes", C.c_int64), ("contexts", C.c_int),
                 ("max_batch", C.c_int), ("max_plans", C.c_int), ("max_inflight", C.c_int),
-                ("max_pending", C.c_int)]
+                ("max_pending", C.c_int), ("solo_bytes", C.c_int64)]
 
 
 class ServeStats(C.Structure):
     _fields_ = [("requests", C.c_int64), ("batches", C.c_int64), ("seconds", C.c_double),
                 ("spmv_per_s", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
-                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("mean_batch", C.c_double)]
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("mean_batch", C.c_double),
+                ("mean_service_ms", C.c_double), ("mean_launch_us", C.c_double)]
 
 
 SERVE_DEVICE_VECTORS = 2     # tc_server_run mode bit: requests carry device x / y

@@ -239,7 +239,7 @@ tc_status tc_plan_check(const tc_plan *p)
 tc_status tc_spmv(const tc_plan *p, const float *d_x, float *d_y, void *stream)
 {
     if (!p || (!d_x && p->N) || (!d_y && p->M)) return fail(TC_ERR_INVALID, "tc_spmv: null argument");
-    return tc::launch_spmv(p->dev_plan(), d_x, d_y, (cudaStream_t)stream);
+    return tc::launch_plan(p, d_x, d_y, (cudaStream_t)stream);
 }
 
 // Copy x in, multiply, copy y out on `stream`, through the plan's staging
@@ -254,7 +254,7 @@ static tc_status spmv_host_enqueue(tc_plan *p, const float *h_x, float *h_y, int
         if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(TC_ERR_ALLOC, "x/y staging buffers");
     }
     if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x, sizeof(float) * (size_t)p->N, cudaMemcpyHostToDevice, s));
-    TC_CHECK(tc::launch_spmv(p->dev_plan(), dx, dy, s));
+    TC_CHECK(tc::launch_plan(p, dx, dy, s));
     if (p->M) TC_CUDA(cudaMemcpyAsync(h_y, dy, sizeof(float) * (size_t)p->M, cudaMemcpyDeviceToHost, s));
     return TC_OK;
 }

@@ -89,19 +89,25 @@ constexpr int kStream4Rows = 1024;    // most rows of a TILE_STREAM4 tile (a run
 constexpr int kDirectRows = 1024;     // most rows of a direct tile (TILE_DIRECT4)
 constexpr int kDirectWideBlock = 1024; // threads of the direct kernel's CTAs
 constexpr int kDirectWideRows = 4 * kDirectWideBlock;   // most rows of a TILE_DIRECT_WIDE tile
+// A wide plan of at most kWideBoundTiles whole tiles passes each tile's
+// first CSR word in the launch parameters (WideBounds), so a CTA loads its
+// tile's words into shared memory (kWideWordQ int4s at most) at the same
+// time as its row pointers instead of after them.
+constexpr int kWideBoundTiles = 1024;
+constexpr int kWideWordQ = 2048;
+struct WideBounds {
+    int nz[kWideBoundTiles + 1];
+};
 
 // Window plans (tc_window.cu): tiles of consecutive rows whose row pointers,
 // CSR words and x window are staged in shared memory by bulk copies.
-constexpr int kWinBlock = 512;        // threads of the window kernel's CTAs (one per SM)
+constexpr int kWinBlock = 1024;       // threads of the window kernel's CTAs (one per SM)
 constexpr int kWinRows = 1024;        // most rows of a window tile
 constexpr int kWinNnz = 8192;         // most CSR words of a window tile
 constexpr int kWinHalo = 4096;        // farthest column - row a window reaches, each side
 constexpr int kWinMaxStages = 4;      // pipeline depth (stages of one CTA)
 constexpr int kWinSmemBudget = 200 * 1024;   // shared memory of the stages
-constexpr int kWinMinRows = 1 << 16;  // smaller matrices keep the one-CTA-per-tile kernels
 constexpr double kWinCover = 0.95;    // share of the in-halo accesses the window range holds
-constexpr double kWinMinShare = 0.5;  // share of all accesses it must hold for a window plan
-constexpr double kWinMinAccesses = 2.0;   // terms per row below which the direct kernels win
 
 // Everything a multiply kernel needs about one plan (passed by value).
 struct DevPlan {
@@ -162,6 +168,7 @@ struct tc_plan {
     // host copies of the small format arrays (always) and optionally the CSR
     std::vector<int> h_xStart, h_yStart, h_xStop, h_nDiasPtr, h_offsets;
     std::vector<int> h_rowptr, h_cols;   // only with TC_FLAG_KEEP_HOST
+    std::vector<int> h_wide_nz;          // wide plans: first CSR word of each tile, and the end
     // partition diagnostics
     double partition_ms = 0.0;
     int thumb_W = 0, thumb_H = 0;
@@ -199,7 +206,11 @@ constexpr int kStreamManyMinBlocks = 8;
 // from memory instead of the parameter bank (48 registers).
 constexpr int kItemMinBlocks = 5;
 // Launch of the multiply kernel for one plan.
-tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s);
+// wb: the tiles' word bounds of a wide plan (nullptr: the kernels that read
+// them from the tile list).  launch_plan passes the plan's own.
+tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s,
+                      const WideBounds *wb = nullptr);
+tc_status launch_plan(const tc_plan *p, const float *x, float *y, cudaStream_t s);
 // Window plans (tc_window.cu): the planner (false when the matrix does not
 // qualify), the kernels' shared-memory setup and the launch.
 bool plan_window(const tc_plan *p, const int *rowptr, const int *cols, std::vector<Tile> &wtiles, int *wlo,

@@ -9,9 +9,9 @@
 // on the GPU and requests are waiting, it packs every waiting request (up to
 // max_batch, and, for host vectors, what fits the context's device arena)
 // into one batch on a free launch context -- the x copies, one multiply
-// launch per word kind over all of the batch's tiles (heterogeneous
-// matrices, the same tile code as tc_spmv, so each y is bit-identical alone
-// and in a mix), the y copies -- and records an event.  So the batch size
+// launch over all of the batch's tiles (heterogeneous matrices, the same
+// tile code as tc_spmv, so each y is bit-identical alone and in a mix), the
+// y copies -- and records an event.  So the batch size
 // follows the load: at a low rate every request launches at once; at a high
 // rate the requests that arrive while batches run are taken together by the
 // next one.  Completion is polled per context; a request's completion time
@@ -54,12 +54,12 @@ struct BatchArgs {
 };
 
 // One CTA per work item (tile, or quarter of a wide direct tile) of the
-// batch's requests whose matrices all have plain (SIGNED = false) or all
-// hybrid words; request i owns items [r[i].tile_begin, r[i + 1].tile_begin).
+// batch's requests; request i owns items [r[i].tile_begin, r[i + 1].tile_begin).
 // Thread 0 finds the CTA's request by binary search and parks its plan
-// descriptor in shared memory.  LEAN: every admitted plan holds only stream,
-// direct and long tiles.
-template <bool SIGNED, bool LEAN>
+// descriptor in shared memory; the CTA then runs the tile code of its plan's
+// word kind (plain or hybrid), so one launch serves every request of the
+// batch.  LEAN: every admitted plan holds only stream, direct and long tiles.
+template <bool LEAN>
 __global__ void __launch_bounds__(kBlock, LEAN ? kItemMinBlocks : 1)
     serve_kernel(const DevPlan *__restrict__ plans, const __grid_constant__ BatchArgs b)
 {
@@ -80,7 +80,8 @@ __global__ void __launch_bounds__(kBlock, LEAN ? kItemMinBlocks : 1)
     __syncthreads();
     const int parts = tile_parts(sp.per_tile);
     const Tile t = sp.tiles[sitem / parts];
-    run_tile_part<SIGNED, LEAN>(sp, t, sitem % parts, sr.x, sr.y, false);
+    if (sp.hybrid) run_tile_part<true, LEAN>(sp, t, sitem % parts, sr.x, sr.y, false);
+    else run_tile_part<false, LEAN>(sp, t, sitem % parts, sr.x, sr.y, false);
 }
 
 double now_s()
@@ -103,6 +104,7 @@ struct tc_server {
         float *arena = nullptr;            // device x / y slots (host-vector requests)
         std::vector<uint64_t> reqs;        // tickets of the batch in flight
         bool busy = false;
+        double t_launch = 0.0;             // when its batch was launched
     };
     std::vector<Ctx> ctx;
     std::vector<tc_plan *> plans;          // admitted (not owned); null = evicted
@@ -138,6 +140,7 @@ struct tc_server {
     std::vector<double> lat_ms;
     int64_t batches = 0, completed = 0;
     double t_first = 0.0, t_last = 0.0;
+    double service_s = 0.0, launch_s = 0.0;   // summed over batches: launch -> seen done, host packing
     std::string worker_error;
 };
 
@@ -162,6 +165,7 @@ void complete_ctx(tc_server *sv, tc_server::Ctx &c, double t, bool ok)
         s.state.store(ok ? tc::kDone : tc::kFailed, std::memory_order_release);
     }
     sv->completed += (int64_t)c.reqs.size();
+    sv->service_s += t - c.t_launch;
     c.reqs.clear();
     c.busy = false;
 }
@@ -172,11 +176,12 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
 {
     *taken = 0;
     const bool dv = sv->mode_device_vectors != 0;
-    tc::BatchArgs args[2];
-    args[0].n = args[1].n = 0;
-    int tiles[2] = {0, 0};
+    tc::BatchArgs args;
+    args.n = 0;
+    int tiles = 0;
     int64_t used = 0;
-    std::vector<std::pair<uint64_t, int>> order;    // ticket, pass
+    std::vector<std::pair<uint64_t, int>> order;    // ticket, 0: shared launch, 1: its own
+    std::vector<tc::ReqDesc> solo;
     while (!pending.empty() && (int)order.size() < sv->cfg.max_batch) {
         const uint64_t tk = pending.front();
         tc_server::Slot &s = sv->slots[tk & (sv->ring - 1)];
@@ -192,32 +197,34 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
             used += need;
             if (p->N) TC_CUDA(cudaMemcpyAsync(ax, s.x, 4 * (size_t)p->N, cudaMemcpyHostToDevice, c.s));
         }
-        const int pass = p->hybrid ? 1 : 0;
-        tc::BatchArgs &a = args[pass];
-        a.r[a.n] = tc::ReqDesc{s.matrix, tiles[pass], dx, dy};
-        tiles[pass] += p->ntiles * tc::tile_parts(p->dev_plan().per_tile);
-        ++a.n;
-        order.emplace_back(tk, pass);
+        if (sv->cfg.solo_bytes > 0 && p->spmv_bytes() >= sv->cfg.solo_bytes) {
+            // a large matrix runs its own multiply kernel (the one tc_spmv
+            // launches) after the batch's shared launches, on the same stream
+            solo.push_back(tc::ReqDesc{s.matrix, 0, dx, dy});
+            order.emplace_back(tk, 1);
+        } else {
+            args.r[args.n] = tc::ReqDesc{s.matrix, tiles, dx, dy};
+            tiles += p->ntiles * tc::tile_parts(p->dev_plan().per_tile);
+            ++args.n;
+            order.emplace_back(tk, 0);
+        }
         s.state.store(tc::kRunning, std::memory_order_relaxed);
         pending.pop_front();
     }
     if (order.empty()) return TC_OK;
     const bool lean = sv->nonlean == 0;
-    if (tiles[0] > 0) {
-        if (lean) tc::serve_kernel<false, true><<<tiles[0], tc::kBlock, 0, c.s>>>(sv->d_plans, args[0]);
-        else tc::serve_kernel<false, false><<<tiles[0], tc::kBlock, 0, c.s>>>(sv->d_plans, args[0]);
-    }
-    if (tiles[1] > 0) {
-        if (lean) tc::serve_kernel<true, true><<<tiles[1], tc::kBlock, 0, c.s>>>(sv->d_plans, args[1]);
-        else tc::serve_kernel<true, false><<<tiles[1], tc::kBlock, 0, c.s>>>(sv->d_plans, args[1]);
+    if (tiles > 0) {
+        if (lean) tc::serve_kernel<true><<<tiles, tc::kBlock, 0, c.s>>>(sv->d_plans, args);
+        else tc::serve_kernel<false><<<tiles, tc::kBlock, 0, c.s>>>(sv->d_plans, args);
     }
     TC_CUDA(cudaGetLastError());
+    for (const tc::ReqDesc &d : solo) TC_CHECK(tc::launch_plan(sv->plans[d.plan], d.x, d.y, c.s));
     if (!dv) {
         int k[2] = {0, 0};
         for (auto &o : order) {
             const tc_server::Slot &s = sv->slots[o.first & (sv->ring - 1)];
             const tc_plan *p = sv->plans[s.matrix];
-            const tc::ReqDesc &d = args[o.second].r[k[o.second]++];
+            const tc::ReqDesc &d = o.second == 1 ? solo[k[1]++] : args.r[k[0]++];
             if (p->M) TC_CUDA(cudaMemcpyAsync(s.y, d.y, 4 * (size_t)p->M, cudaMemcpyDeviceToHost, c.s));
         }
     }
@@ -264,7 +271,9 @@ void dispatcher(tc_server *sv, int device)
                 if (!c.busy) { fc = &c; break; }
             if (!fc) break;
             int taken = 0;
+            const double tl = tc::now_s();
             const tc_status st = launch_batch(sv, *fc, pending, &taken);
+            fc->t_launch = tl;
             if (st != TC_OK) {
                 sv->worker_error = tc_last_error();
                 sv->worker_status.store(st);
@@ -278,6 +287,7 @@ void dispatcher(tc_server *sv, int device)
             {
                 std::lock_guard<std::mutex> lk(sv->st_mu);
                 ++sv->batches;
+                sv->launch_s += tc::now_s() - tl;
             }
             idle = false;
         }
@@ -318,6 +328,7 @@ void tc_serve_config_default(tc_serve_config *c)
     c->max_plans = 1024;
     c->max_inflight = 2;
     c->max_pending = 1 << 16;
+    c->solo_bytes = 0;
 }
 
 tc_status tc_server_create(const tc_serve_config *cfg, tc_server **out)
@@ -429,6 +440,7 @@ tc_status tc_server_start(tc_server *sv, int device_vectors)
         sv->lat_ms.clear();
         sv->batches = sv->completed = 0;
         sv->t_first = sv->t_last = 0.0;
+        sv->service_s = sv->launch_s = 0.0;
     }
     sv->running.store(true);
     try {
@@ -519,7 +531,7 @@ tc_status tc_server_wait(tc_server *sv, uint64_t ticket, double timeout_s)
 }
 
 static void fill_stats(tc_server *sv, const std::vector<double> &lat, double seconds, int64_t batches,
-                       tc_serve_stats *stats)
+                       tc_serve_stats *stats, double service_s = 0.0, double launch_s = 0.0)
 {
     memset(stats, 0, sizeof *stats);
     const size_t n = lat.size();
@@ -539,6 +551,8 @@ static void fill_stats(tc_server *sv, const std::vector<double> &lat, double sec
         stats->mean_ms = sum / n;
     }
     stats->mean_batch = batches ? (double)n / batches : 0.0;
+    stats->mean_service_ms = batches ? 1e3 * service_s / batches : 0.0;
+    stats->mean_launch_us = batches ? 1e6 * launch_s / batches : 0.0;
     (void)sv;
 }
 
@@ -546,7 +560,8 @@ tc_status tc_server_stats(tc_server *sv, tc_serve_stats *stats)
 {
     if (!sv || !stats) return fail(TC_ERR_INVALID, "tc_server_stats: null argument");
     std::lock_guard<std::mutex> lk(sv->st_mu);
-    fill_stats(sv, sv->lat_ms, sv->t_last > sv->t_first ? sv->t_last - sv->t_first : 0.0, sv->batches, stats);
+    fill_stats(sv, sv->lat_ms, sv->t_last > sv->t_first ? sv->t_last - sv->t_first : 0.0, sv->batches, stats,
+               sv->service_s, sv->launch_s);
     return TC_OK;
 }
 
@@ -575,7 +590,7 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
     const bool device_vectors = (mode & TC_SERVE_DEVICE_VECTORS) != 0;
     std::vector<double> done(nreq, 0.0);
     int64_t batches = 0;
-    double t0 = 0.0;
+    double t0 = 0.0, service_s = 0.0, launch_s = 0.0;
 
     if (mode & 1) {    // plain: one synchronous request at a time on this thread
         tc_server::Ctx &c = sv->ctx[0];
@@ -612,6 +627,8 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
         for (int r = 0; r < nreq; ++r) done[r] = tdone[r] > 0 ? tdone[r] - t0 : 0.0;
         std::lock_guard<std::mutex> lk(sv->st_mu);
         batches = sv->batches;
+        service_s = sv->service_s;
+        launch_s = sv->launch_s;
     }
     // statistics: latency = completion - arrival
     std::vector<double> lat(nreq);
@@ -622,7 +639,7 @@ tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const 
         first = std::min(first, arrival_s[r]);
         last = std::max(last, done[r]);
     }
-    if (stats) fill_stats(sv, lat, last - first, batches, stats);
+    if (stats) fill_stats(sv, lat, last - first, batches, stats, service_s, launch_s);
     return TC_OK;
 }
 

@@ -251,6 +251,34 @@ __global__ void __launch_bounds__(kBlock, LEAN ? (SIGNED ? kLeanMinBlocksSigned 
     }
 }
 
+// The whole-tile wide kernel with the tiles' word bounds in the launch
+// parameters: each CTA reads its tile's CSR words into shared memory with
+// coalesced int4 loads issued together with its row-pointer loads, so the
+// chain before the gathers is one memory round trip instead of two (row
+// pointers, then the words they point to).  Same runs, terms and order as
+// spmv_wide_kernel<SIGNED, true>.
+template <bool SIGNED>
+__global__ void __launch_bounds__(kDirectWideBlock, 2)
+    spmv_wide_bounds_kernel(DevPlan p, const __grid_constant__ WideBounds tb, const float *__restrict__ x,
+                            float *__restrict__ y)
+{
+    __shared__ int4 sw[kWideWordQ];
+    allow_next_grid();
+    const int row0 = blockIdx.x * kDirectWideRows;
+    const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+    if (threadIdx.x == 0) prefetch_l2(x + row0, kDirectWideRows * sizeof(float));
+    const int nz0 = tb.nz[blockIdx.x], nz1 = tb.nz[blockIdx.x + 1];
+    const int base = nz0 & ~3;
+    const int nq = min((nz1 - base + 3) >> 2, kWideWordQ);
+    const int4 *cq = reinterpret_cast<const int4 *>(p.cols + base);
+    for (int i = threadIdx.x; i < nq; i += kDirectWideBlock) sw[i] = __ldg(cq + i);
+    const int g = row0 + 4 * threadIdx.x;
+    const int4 r4 = __ldg(reinterpret_cast<const int4 *>(p.rowptr + g));
+    const int e4 = __ldg(p.rowptr + g + 4);
+    __syncthreads();
+    direct_run_staged<SIGNED>(p, dc, x, y, g, r4, e4, reinterpret_cast<const int *>(sw), base, 4 * nq);
+}
+
 // The multiply of a plan of stream tiles only (meshes, banded and other
 // matrices of short, even rows): the grid kernel with no code for the other
 // tile kinds.  MANY: more tiles than one wave, compiled for 8 CTAs per SM.
@@ -387,7 +415,7 @@ size_t stream_smem_bytes(const DevPlan &dp)
 }
 
 template <bool SIGNED>
-static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaStream_t s)
+static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const float *x, float *y, cudaStream_t s)
 {
     if (dp.ntiles <= 0) return TC_OK;
     const size_t smem = dp.per_tile ? 0 : stream_smem_bytes(dp);
@@ -404,7 +432,9 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
     cfg.numAttrs = 1;
     const bool full = dp.M % kDirectWideRows == 0 && dp.N >= dp.M &&
                       ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
-    if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
+    if (dp.per_tile == 3 && full && wb)
+        TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_bounds_kernel<SIGNED>, dp, *wb, x, y));
+    else if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, false>, dp, x, y));
     else if (dp.per_tile == 4 && dp.ntiles > kLeanMinBlocks * num_sms())
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_stream_kernel<SIGNED, true>, dp, x, y));
@@ -415,11 +445,19 @@ static tc_status launch_tiles(const DevPlan &dp, const float *x, float *y, cudaS
     return TC_OK;
 }
 
-tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s)
+tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s, const WideBounds *wb)
 {
     if (dp.M == 0) return TC_OK;
     if (dp.nwtiles > 0) return launch_window(dp, x, y, s);
-    return dp.hybrid ? launch_tiles<true>(dp, x, y, s) : launch_tiles<false>(dp, x, y, s);
+    return dp.hybrid ? launch_tiles<true>(dp, wb, x, y, s) : launch_tiles<false>(dp, wb, x, y, s);
+}
+
+tc_status launch_plan(const tc_plan *p, const float *x, float *y, cudaStream_t s)
+{
+    if (p->h_wide_nz.empty()) return launch_spmv(p->dev_plan(), x, y, s, nullptr);
+    WideBounds wb;
+    memcpy(wb.nz, p->h_wide_nz.data(), sizeof(int) * p->h_wide_nz.size());
+    return launch_spmv(p->dev_plan(), x, y, s, &wb);
 }
 
 tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,
@@ -538,6 +576,12 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     }
     p->ntiles = (int)tiles.size();
     p->nnz_csr = csrRow[M];
+    p->h_wide_nz.clear();
+    if (p->ntiles_wide == p->ntiles && p->ntiles > 0 && p->ntiles <= kWideBoundTiles &&
+        M % kDirectWideRows == 0 && !(p->params.flags & TC_FLAG_NO_BOUNDS)) {
+        for (const Tile &t : tiles) p->h_wide_nz.push_back(t.nz0);
+        p->h_wide_nz.push_back(csrRow[M]);
+    }
     // shared-memory stage sizes (ints, multiples of 4) from the largest tile
     int max_rows = 1, max_nnz = 0;
     for (const Tile &t : tiles)

@@ -479,6 +479,54 @@ __device__ __forceinline__ float diag_tile_row(const DevPlan &p, const float *__
     return acc;
 }
 
+// The x segment of a one-shape tile's dense diagonals, staged in shared
+// memory while the tile's CSR gathers are in flight: for rows [row0, row0 +
+// nr) of shape s with offsets lo..hi (ascending), every diagonal term reads
+// column row + (yStart - xStart) + off, all inside [row0 + cb + lo, row0 +
+// nr - 1 + cb + hi].  Loaded with consecutive threads on consecutive columns
+// (coalesced) after the wait, it turns the rows' diagonal terms into shared-
+// memory reads; the sum keeps diag_tile_row's terms and order.
+constexpr int kDiagWin = 1536;     // floats of the staged segment (longer: no staging)
+
+__device__ __forceinline__ float *diag_smem()
+{
+    __shared__ float xs[kDiagWin];
+    return xs;
+}
+
+// Stages the segment of tile rows [row0, row0 + nr) of class dc when the
+// class names one shape and the segment fits (uniform across the CTA);
+// issued after the wait and completed by the caller's next barrier.
+// Returns whether it staged.
+__device__ __forceinline__ bool diag_seg_stage(const DevPlan &p, int dc, int row0, int nr,
+                                               const float *__restrict__ x)
+{
+    if (dc == kDiagNone || dc == kDiagGeneral) return false;
+    const int4 sh = __ldg(p.shapes + dc - 1);
+    const int2 dr = __ldg(p.shape_dias + dc - 1);
+    const int lo = __ldg(p.offsets + dr.x), hi = __ldg(p.offsets + dr.y - 1);
+    const int len = nr + hi - lo;
+    if (len > kDiagWin) return false;
+    const int first = row0 + sh.z - sh.x + lo;
+    float *xs = diag_smem();
+    for (int i = threadIdx.x; i < len; i += kBlock) {
+        const int c = first + i;
+        xs[i] = c >= 0 && c < p.N ? ldx(x + c) : 0.f;
+    }
+    return true;
+}
+
+// The dense-diagonal terms of tile row rl of a staged tile of class dc, in
+// offset order (the shape record and offsets are re-read: L1 hits).
+__device__ __forceinline__ float diag_seg_row(const DevPlan &p, int dc, int rl)
+{
+    const int2 dr = __ldg(p.shape_dias + dc - 1);
+    const float *xs = diag_smem() + rl - __ldg(p.offsets + dr.x);
+    float acc = 0.f;
+    for (int d = dr.x; d < dr.y; ++d) acc += xs[__ldg(p.offsets + d)];
+    return acc;
+}
+
 template <bool SIGNED>
 __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__restrict__ x,
                             float *__restrict__ y, bool wait)
@@ -498,14 +546,13 @@ __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__rest
         re[k] = ok ? __ldg(p.rowptr + row0 + rl + 1) - base : 0;
     }
     if (wait) wait_prior_grid(x, y);
-    stream_gather<SIGNED>(x, vals, sw);
-    // (Loading the rows' diagonal terms while the gathers are in flight
-    // measured slower on the mesh, 69.5 against 65.6 µs.)
+    const bool seg = SIGNED && diag_seg_stage(p, dc, row0, nr, x);
+    stream_gather<SIGNED>(x, vals, sw);                         // ends with a barrier
 #pragma unroll
     for (int k = 0; k < RQ; ++k) {
         const int rl = tid + k * kBlock;
         if (rl < nr) {
-            float acc = diag_tile_row(p, x, dc, row0 + rl);
+            float acc = seg ? diag_seg_row(p, dc, rl) : diag_tile_row(p, x, dc, row0 + rl);
             for (int j = rb[k]; j < re[k]; ++j) acc += vals[j];
             y[row0 + rl] = acc;
         }
@@ -536,7 +583,8 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
         rp4[k] = ok ? __ldg(p.rowptr + row0 + min(g + 4, nr)) : 0;
     }
     if (wait) wait_prior_grid(x, y);
-    stream_gather<SIGNED>(x, vals, sw);
+    const bool seg = SIGNED && diag_seg_stage(p, dc, row0, nr, x);
+    stream_gather<SIGNED>(x, vals, sw);                         // ends with a barrier
 #pragma unroll
     for (int k = 0; k < GQ; ++k) {
         const int g = 4 * (tid + k * kBlock);
@@ -547,7 +595,7 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
         for (int u = 0; u < 4; ++u) {
             acc[u] = 0.f;
             if (g + u < nr) {
-                acc[u] = diag_tile_row(p, x, dc, row0 + g + u);
+                acc[u] = seg ? diag_seg_row(p, dc, g + u) : diag_tile_row(p, x, dc, row0 + g + u);
                 const int e = g + u + 1 < nr ? b[u + 1] : b[4];
                 for (int j = b[u]; j < e; ++j) acc[u] += vals[j];
             }
@@ -683,6 +731,41 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
             if (b[0] + w >= b[u] && b[0] + w < b[u + 1]) acc[u] += v[w];
     for (int j = b[0] + kDirectW; j < e4; ++j) {
         const float z = gather<SIGNED>(x, __ldg(p.cols + j));
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (j >= b[u] && j < b[u + 1]) acc[u] += z;
+    }
+    *reinterpret_cast<float4 *>(y + g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+}
+
+// direct_run_full with the tile's CSR words already in shared memory: ws[k]
+// = cols[base + k] for k < lim (the words past lim, if any, from global
+// memory).  The row pointers r4 / e4 of the run were loaded by the caller.
+template <bool SIGNED>
+__device__ __forceinline__ void direct_run_staged(const DevPlan &p, int dc, const float *__restrict__ x,
+                                                  float *__restrict__ y, int g, int4 r4, int e4,
+                                                  const int *ws, int base, int lim)
+{
+    const int b[5] = {r4.x, r4.y, r4.z, r4.w, e4};
+    int c[kDirectW];
+#pragma unroll
+    for (int w = 0; w < kDirectW; ++w) {
+        const int j = b[0] + w;
+        c[w] = j < e4 ? (j - base < lim ? ws[j - base] : __ldg(p.cols + j)) : 0;
+    }
+    wait_prior_grid(x, y);
+    float v[kDirectW];
+#pragma unroll
+    for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    if (SIGNED) diag_run4(p, x, dc, g, 4, acc);
+#pragma unroll
+    for (int w = 0; w < kDirectW; ++w)
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (b[0] + w >= b[u] && b[0] + w < b[u + 1]) acc[u] += v[w];
+    for (int j = b[0] + kDirectW; j < e4; ++j) {
+        const float z = gather<SIGNED>(x, j - base < lim ? ws[j - base] : __ldg(p.cols + j));
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (j >= b[u] && j < b[u + 1]) acc[u] += z;

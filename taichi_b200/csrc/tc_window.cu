@@ -77,6 +77,17 @@ __device__ __forceinline__ void win_issue_x(const DevPlan &p, const Tile &t, int
     if (wlen) bulk_load(st + p.w_rp + p.w_cw, x + wa, 4u * (unsigned)wlen, bar);
 }
 
+// A coherent load of x that the compiler may not execute speculatively: the
+// global read of an out-of-window column must stay on its branch (a load
+// the compiler takes for side-effect free may be if-converted and issued for
+// every term, window hits included).
+__device__ __forceinline__ float ldx_guarded(const float *p)
+{
+    float v;
+    asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // x[c] from the staged window when c lies in it, else from global memory.
 struct WinX {
     const float *xw;
@@ -86,7 +97,8 @@ struct WinX {
     __device__ __forceinline__ float operator()(int c) const
     {
         const unsigned k = (unsigned)(c - wa);
-        return k < wlen ? xw[k] : ldx(x + c);
+        if (k < wlen) return xw[k];
+        return ldx_guarded(x + c);
     }
 };
 
@@ -250,12 +262,9 @@ tc_status launch_window(const DevPlan &dp, const float *x, float *y, cudaStream_
 
 // ------------------------------------------------------------------ planner
 // Window offsets [wlo, whi] of a plan: the shortest range of column - row
-// that holds at least kWinCover of the matrix's accesses within
-// +-kWinHalo (dense-diagonal terms and CSR words, rows sampled evenly when
-// the matrix is large).  The plan runs window tiles when that range holds at
-// least kWinMinShare of all its accesses and the rows average at least
-// kWinMinAccesses terms (sparser matrices keep the direct kernels), unless a
-// flag forces or forbids it.
+// that holds at least kWinCover of the matrix's accesses within +-kWinHalo
+// (dense-diagonal terms and CSR words, rows sampled evenly when the matrix is
+// large).  Built only on request (TC_FLAG_WINDOW).
 bool plan_window(const tc_plan *p, const int *rp, const int *cw, std::vector<Tile> &wt, int *wlo, int *whi,
                  int *max_rows, int *max_nnz)
 {
@@ -264,7 +273,11 @@ bool plan_window(const tc_plan *p, const int *rp, const int *cw, std::vector<Til
     const int flags = p->params.flags;
     const bool force = (flags & TC_FLAG_WINDOW) != 0;
     if (p->params.tile_mode != 2 || (flags & TC_FLAG_NO_WINDOW) || M == 0) return false;
-    if (!force && M < kWinMinRows) return false;
+    // Only on request (the flag, or the tuner when it times the window plan
+    // faster): on the 9-point mesh (2048^2) the window kernel measured 108 us
+    // per multiply against 52 us for the stream tiles, whose CTA-per-tile
+    // grid keeps more loads in flight than one pipelined CTA per SM.
+    if (!force) return false;
     const int H = kWinHalo;
     std::vector<int64_t> hist(2 * H + 1, 0);
     int64_t total = 0;
@@ -307,11 +320,6 @@ bool plan_window(const tc_plan *p, const int *rp, const int *cw, std::vector<Til
         }
         sum -= hist[lo];
     }
-    int64_t covered = 0;
-    for (int k = best_lo; k <= best_hi; ++k) covered += hist[k];
-    if (!force && ((double)covered < kWinMinShare * (double)total ||
-                   (double)total < kWinMinAccesses * (double)rows_seen))
-        return false;
     *wlo = best_lo - H;
     *whi = best_hi - H;
     const int rows_cap = std::max(1, std::min(p->params.tile_rows, kWinRows));

@@ -30,11 +30,14 @@ def solo(plan, x, M, dev):
     return y.cpu().numpy()
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3], ids=["batched", "plain", "batched_dev", "plain_dev"])
-def test_served_results_identical_to_solo(tc, dev, mode):
+@pytest.mark.parametrize("mode,solo_bytes", [(0, 0), (1, 0), (2, 0), (3, 0), (0, 1), (2, 1)],
+                         ids=["batched", "plain", "batched_dev", "plain_dev", "batched_solo", "batched_dev_solo"])
+def test_served_results_identical_to_solo(tc, dev, mode, solo_bytes):
+    """solo_bytes = 1: every matrix counts as large, so each request runs its own
+    multiply launch inside its batch (the path of large matrices)."""
     import torch
     plans, mats = make_plans(tc)
-    srv = tc.Server(contexts=3, max_batch=32, arena_bytes=64 << 20)
+    srv = tc.Server(contexts=3, max_batch=32, arena_bytes=64 << 20, solo_bytes=solo_bytes)
     ids = [srv.admit(p) for p in plans]
     rng = np.random.default_rng(3 + mode)
     n = 300

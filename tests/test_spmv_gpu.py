@@ -334,22 +334,22 @@ def test_spmv_mesh2048_full_size(tc, dev):
     (37.7 M non-zeros, the one plain configuration larger than L2), formatted
     by the GPU partitioner (whose format equals the reference's for this
     matrix, see test_partition_gpu): integer x exact, x = 1, FP32 x within
-    1e-5 of FP64 normwise and per row.  The default plan is a window plan;
-    the stream-tile plan of the same format gives the same y bit for bit."""
+    1e-5 of FP64 normwise and per row.  The window plan of the same format
+    gives the same y bit for bit."""
     case = next(c for c in cases.MATRIX_CASES if c["name"] == "mesh2048")
     M, N, rp, col = cases.matrix(case)
     plan = tc.Plan.from_csr(M, N, rp, col)
     info = plan.info()
-    assert info["dia_shapes"] == 1 and info["nwtiles"] > 0, info
+    assert info["dia_shapes"] == 1 and info["nwtiles"] == 0, info
     fmt = plan.export()
-    check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/window")
-    x = np.random.default_rng(17).uniform(-1, 1, N).astype(np.float32)
-    y_win = run_spmv(plan, x, M, dev)
-    plan.close()
-    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW))
-    assert plan.info()["nwtiles"] == 0
     check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/stream")
-    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_win)
+    x = np.random.default_rng(17).uniform(-1, 1, N).astype(np.float32)
+    y_stream = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=tc.TC_FLAG_WINDOW))
+    assert plan.info()["nwtiles"] > 0
+    check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/window")
+    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_stream)
     plan.close()
 
 
@@ -401,27 +401,51 @@ def test_window_unaligned_vectors(tc, dev):
 
 
 def test_window_plan_selection(tc, dev):
-    """The planner picks a window plan for a mesh and banded matrices, and
-    not for an R-MAT graph (rows averaging under one entry) or a small
-    matrix; TC_FLAG_NO_WINDOW turns it off."""
-    M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=1)
-    plan = tc.Plan.from_csr(M, N, rp, col)
+    """Window plans are built on request only (TC_FLAG_WINDOW; the tuner
+    tries them): a mesh gets the window covering its stencil columns, a
+    banded matrix a narrow one; without the flag, or with TC_FLAG_NO_WINDOW
+    as well, no window plan."""
+    W = tc.params(flags=tc.TC_FLAG_WINDOW)
+    M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=1)     # stencil columns r +- 511..513
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=W)
     i = plan.info()
-    assert i["nwtiles"] > 0 and i["window_lo"] <= -2049 and i["window_hi"] >= 2049, i
+    assert i["nwtiles"] > 0 and -1024 < i["window_lo"] <= -513 and 513 <= i["window_hi"] < 1024, i
+    plan.close()
+    plan = tc.Plan.from_csr(M, N, rp, col)
+    assert plan.info()["nwtiles"] == 0
     plan.close()
     rp, col = tc.gen_banded(300000, 4, 3, seed=2)
-    plan = tc.Plan.from_csr(300000, 300000, rp, col)
+    plan = tc.Plan.from_csr(300000, 300000, rp, col, prm=tc.params(flags=tc.TC_FLAG_WINDOW))
     i = plan.info()
     assert i["nwtiles"] > 0 and i["window_lo"] >= -64 and i["window_hi"] <= 64, i
     plan.close()
-    plan = tc.Plan.from_csr(300000, 300000, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW))
+    plan = tc.Plan.from_csr(300000, 300000, rp, col,
+                            prm=tc.params(flags=tc.TC_FLAG_WINDOW | tc.TC_FLAG_NO_WINDOW))
     assert plan.info()["nwtiles"] == 0
     plan.close()
-    M, rp, col = tc.gen_rmat(18, 16, 0.499, 0.001, 0.001, seed=1)
-    plan = tc.Plan.from_csr(M, M, rp, col)
-    assert plan.info()["nwtiles"] == 0
-    plan.close()
-    M, N, rp, col = cases.matrix(next(c for c in cases.MATRIX_CASES if c["name"] == "band_holes"))
-    plan = tc.Plan.from_csr(M, N, rp, col)
-    assert plan.info()["nwtiles"] == 0                      # 20,000 rows: below the window minimum
-    plan.close()
+
+
+def test_wide_bounds_kernel(tc, dev):
+    """Whole wide tiles take their word ranges from the launch parameters
+    and stage their words in shared memory: the same y, bit for bit, as the
+    kernel that reads them through the row pointers (TC_FLAG_NO_BOUNDS), on
+    an R-MAT graph and on a matrix whose first tile holds more words than
+    the shared-memory stage (the rest come from global memory); both against
+    the oracle."""
+    M, rp, col = tc.gen_rmat(16, 16, 0.499, 0.001, 0.001, seed=4)
+    cases_ = [("rmat16", M, rp, col)]
+    M2 = 16384
+    lengths = np.zeros(M2, np.int64)
+    lengths[:4096] = 3                      # 12,288 words in tile 0 (stage: 8,192)
+    rp2, col2 = csr_from_lengths(lengths, M2, 12)
+    cases_.append(("overfull", M2, rp2, col2))
+    x = np.random.default_rng(6).uniform(-1, 1, M2 * 4).astype(np.float32)
+    for name, M, rp, col in cases_:
+        plan = tc.Plan.from_csr(M, M, rp, col, partition=False)
+        assert plan.info()["ntiles"] == M // 4096
+        check_plan(plan, dict(dense_nnz=0), M, M, rp, col, dev, "bounds/" + name)
+        y1 = run_spmv(plan, x[:M], M, dev)
+        plan.close()
+        plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_BOUNDS), partition=False)
+        np.testing.assert_array_equal(run_spmv(plan, x[:M], M, dev), y1, err_msg=name)
+        plan.close()
