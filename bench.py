@@ -208,8 +208,8 @@ def run_ours(args, rank, world, local_rank):
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_WINDOW
     if args.window:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WINDOW
-    if args.no_bounds:
-        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_BOUNDS
+    if args.wide_bounds:
+        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_BOUNDS
     if args.tile_nnz is not None:
         over["tile_nnz"] = args.tile_nnz
     if args.ctas_per_sm is not None:
@@ -654,8 +654,8 @@ def main():
     ap.add_argument("--no-direct", action="store_true", help="stream tiles only, no direct tiles")
     ap.add_argument("--no-window", action="store_true", help="never the window kernel")
     ap.add_argument("--window", action="store_true", help="the window kernel wherever rows fit its tiles")
-    ap.add_argument("--no-bounds", action="store_true",
-                    help="wide plans: the kernel that reads tile word ranges from the tile list")
+    ap.add_argument("--wide-bounds", action="store_true",
+                    help="wide plans: tile word ranges in the launch parameters, words staged in shared memory")
     ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")
     ap.add_argument("--serve-max-batch", type=int, default=64, help="served form: most requests per launch")
     ap.add_argument("--serve-inflight", type=int, default=2, help="served form: batches on the GPU at once")

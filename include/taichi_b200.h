@@ -78,9 +78,11 @@ typedef struct tc_params {
 #define TC_FLAG_NO_WINDOW    0x40 /* tile_mode 2: never run the window kernel
                                      (x staged in shared memory per tile of
                                      rows), even for a banded matrix        */
-#define TC_FLAG_NO_BOUNDS    0x100 /* wide plans: the kernel that reads each
-                                     tile's word range from the tile list
-                                     (not from the launch parameters)       */
+#define TC_FLAG_WIDE_BOUNDS  0x100 /* wide plans of whole tiles: pass each
+                                     tile's word range in the launch
+                                     parameters and stage its words in
+                                     shared memory (off by default: measured
+                                     slower on R-MAT scale 20)              */
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */

@@ -24,7 +24,7 @@ TC_FLAG_NO_DIRECT = 0x10
 TC_FLAG_NO_WIDE = 0x20
 TC_FLAG_NO_WINDOW = 0x40
 TC_FLAG_WINDOW = 0x80
-TC_FLAG_NO_BOUNDS = 0x100
+TC_FLAG_WIDE_BOUNDS = 0x100
 
 _IP = C.POINTER(C.c_int)
 

@@ -578,7 +578,7 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     p->nnz_csr = csrRow[M];
     p->h_wide_nz.clear();
     if (p->ntiles_wide == p->ntiles && p->ntiles > 0 && p->ntiles <= kWideBoundTiles &&
-        M % kDirectWideRows == 0 && !(p->params.flags & TC_FLAG_NO_BOUNDS)) {
+        M % kDirectWideRows == 0 && (p->params.flags & TC_FLAG_WIDE_BOUNDS)) {
         for (const Tile &t : tiles) p->h_wide_nz.push_back(t.nz0);
         p->h_wide_nz.push_back(csrRow[M]);
     }

@@ -479,54 +479,6 @@ __device__ __forceinline__ float diag_tile_row(const DevPlan &p, const float *__
     return acc;
 }
 
-// The x segment of a one-shape tile's dense diagonals, staged in shared
-// memory while the tile's CSR gathers are in flight: for rows [row0, row0 +
-// nr) of shape s with offsets lo..hi (ascending), every diagonal term reads
-// column row + (yStart - xStart) + off, all inside [row0 + cb + lo, row0 +
-// nr - 1 + cb + hi].  Loaded with consecutive threads on consecutive columns
-// (coalesced) after the wait, it turns the rows' diagonal terms into shared-
-// memory reads; the sum keeps diag_tile_row's terms and order.
-constexpr int kDiagWin = 1536;     // floats of the staged segment (longer: no staging)
-
-__device__ __forceinline__ float *diag_smem()
-{
-    __shared__ float xs[kDiagWin];
-    return xs;
-}
-
-// Stages the segment of tile rows [row0, row0 + nr) of class dc when the
-// class names one shape and the segment fits (uniform across the CTA);
-// issued after the wait and completed by the caller's next barrier.
-// Returns whether it staged.
-__device__ __forceinline__ bool diag_seg_stage(const DevPlan &p, int dc, int row0, int nr,
-                                               const float *__restrict__ x)
-{
-    if (dc == kDiagNone || dc == kDiagGeneral) return false;
-    const int4 sh = __ldg(p.shapes + dc - 1);
-    const int2 dr = __ldg(p.shape_dias + dc - 1);
-    const int lo = __ldg(p.offsets + dr.x), hi = __ldg(p.offsets + dr.y - 1);
-    const int len = nr + hi - lo;
-    if (len > kDiagWin) return false;
-    const int first = row0 + sh.z - sh.x + lo;
-    float *xs = diag_smem();
-    for (int i = threadIdx.x; i < len; i += kBlock) {
-        const int c = first + i;
-        xs[i] = c >= 0 && c < p.N ? ldx(x + c) : 0.f;
-    }
-    return true;
-}
-
-// The dense-diagonal terms of tile row rl of a staged tile of class dc, in
-// offset order (the shape record and offsets are re-read: L1 hits).
-__device__ __forceinline__ float diag_seg_row(const DevPlan &p, int dc, int rl)
-{
-    const int2 dr = __ldg(p.shape_dias + dc - 1);
-    const float *xs = diag_smem() + rl - __ldg(p.offsets + dr.x);
-    float acc = 0.f;
-    for (int d = dr.x; d < dr.y; ++d) acc += xs[__ldg(p.offsets + d)];
-    return acc;
-}
-
 template <bool SIGNED>
 __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__restrict__ x,
                             float *__restrict__ y, bool wait)
@@ -546,13 +498,15 @@ __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__rest
         re[k] = ok ? __ldg(p.rowptr + row0 + rl + 1) - base : 0;
     }
     if (wait) wait_prior_grid(x, y);
-    const bool seg = SIGNED && diag_seg_stage(p, dc, row0, nr, x);
-    stream_gather<SIGNED>(x, vals, sw);                         // ends with a barrier
+    stream_gather<SIGNED>(x, vals, sw);
+    // (Loading the rows' diagonal terms while the gathers are in flight
+    // measured slower on the mesh: into registers 69.5 against 65.6 us; as
+    // the tile's x segment staged in shared memory 58.3 against 52.5 us.)
 #pragma unroll
     for (int k = 0; k < RQ; ++k) {
         const int rl = tid + k * kBlock;
         if (rl < nr) {
-            float acc = seg ? diag_seg_row(p, dc, rl) : diag_tile_row(p, x, dc, row0 + rl);
+            float acc = diag_tile_row(p, x, dc, row0 + rl);
             for (int j = rb[k]; j < re[k]; ++j) acc += vals[j];
             y[row0 + rl] = acc;
         }
@@ -583,8 +537,7 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
         rp4[k] = ok ? __ldg(p.rowptr + row0 + min(g + 4, nr)) : 0;
     }
     if (wait) wait_prior_grid(x, y);
-    const bool seg = SIGNED && diag_seg_stage(p, dc, row0, nr, x);
-    stream_gather<SIGNED>(x, vals, sw);                         // ends with a barrier
+    stream_gather<SIGNED>(x, vals, sw);
 #pragma unroll
     for (int k = 0; k < GQ; ++k) {
         const int g = 4 * (tid + k * kBlock);
@@ -595,7 +548,7 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
         for (int u = 0; u < 4; ++u) {
             acc[u] = 0.f;
             if (g + u < nr) {
-                acc[u] = seg ? diag_seg_row(p, dc, g + u) : diag_tile_row(p, x, dc, row0 + g + u);
+                acc[u] = diag_tile_row(p, x, dc, row0 + g + u);
                 const int e = g + u + 1 < nr ? b[u + 1] : b[4];
                 for (int j = b[u]; j < e; ++j) acc[u] += vals[j];
             }

@@ -426,9 +426,9 @@ def test_window_plan_selection(tc, dev):
 
 
 def test_wide_bounds_kernel(tc, dev):
-    """Whole wide tiles take their word ranges from the launch parameters
-    and stage their words in shared memory: the same y, bit for bit, as the
-    kernel that reads them through the row pointers (TC_FLAG_NO_BOUNDS), on
+    """Whole wide tiles taking their word ranges from the launch parameters
+    and staging their words in shared memory (TC_FLAG_WIDE_BOUNDS): the same
+    y, bit for bit, as the kernel that reads them through the row pointers, on
     an R-MAT graph and on a matrix whose first tile holds more words than
     the shared-memory stage (the rest come from global memory); both against
     the oracle."""
@@ -441,11 +441,11 @@ def test_wide_bounds_kernel(tc, dev):
     cases_.append(("overfull", M2, rp2, col2))
     x = np.random.default_rng(6).uniform(-1, 1, M2 * 4).astype(np.float32)
     for name, M, rp, col in cases_:
-        plan = tc.Plan.from_csr(M, M, rp, col, partition=False)
+        plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_WIDE_BOUNDS), partition=False)
         assert plan.info()["ntiles"] == M // 4096
         check_plan(plan, dict(dense_nnz=0), M, M, rp, col, dev, "bounds/" + name)
         y1 = run_spmv(plan, x[:M], M, dev)
         plan.close()
-        plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_BOUNDS), partition=False)
+        plan = tc.Plan.from_csr(M, M, rp, col, partition=False)
         np.testing.assert_array_equal(run_spmv(plan, x[:M], M, dev), y1, err_msg=name)
         plan.close()
