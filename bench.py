@@ -208,6 +208,8 @@ def run_ours(args, rank, world, local_rank):
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_NO_WINDOW
     if args.window:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WINDOW
+    if args.wide_fixed:
+        over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_FIXED
     if args.wide_bounds:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_BOUNDS
     if args.tile_nnz is not None:
@@ -654,12 +656,14 @@ def main():
     ap.add_argument("--no-direct", action="store_true", help="stream tiles only, no direct tiles")
     ap.add_argument("--no-window", action="store_true", help="never the window kernel")
     ap.add_argument("--window", action="store_true", help="the window kernel wherever rows fit its tiles")
+    ap.add_argument("--wide-fixed", action="store_true",
+                    help="wide plans: tiles of 4096 rows instead of two equal tiles per SM")
     ap.add_argument("--wide-bounds", action="store_true",
                     help="wide plans: tile word ranges in the launch parameters, words staged in shared memory")
     ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")
     ap.add_argument("--serve-max-batch", type=int, default=64, help="served form: most requests per launch")
     ap.add_argument("--serve-inflight", type=int, default=2, help="served form: batches on the GPU at once")
-    ap.add_argument("--serve-solo-mb", type=float, default=0.0,
+    ap.add_argument("--serve-solo-mb", type=float, default=16.0,
                     help="served form: matrices moving at least this many MB per SpMV get their own launch")
     ap.add_argument("--rate-search", type=int, default=4,
                     help="served form: bisection steps between the last passing and first failing rate")

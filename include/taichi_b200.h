@@ -83,6 +83,8 @@ typedef struct tc_params {
                                      parameters and stage its words in
                                      shared memory (off by default: measured
                                      slower on R-MAT scale 20)              */
+#define TC_FLAG_WIDE_FIXED   0x200 /* wide plans: tiles of 4096 rows
+                                     instead of two equal tiles per SM     */
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */
@@ -326,8 +328,8 @@ typedef struct tc_serve_config {
     int max_pending;      /* online requests outstanding at once (65536)         */
     int64_t solo_bytes;   /* a request whose matrix moves at least this many
                              bytes per SpMV runs its own multiply launch (the
-                             kernel tc_spmv picks) inside its batch instead of
-                             sharing the batch's launch (0: never, the default) */
+                             kernel tc_spmv picks) on a second stream beside
+                             its batch's shared launch (16 MiB; 0: never)       */
 } tc_serve_config;
 
 typedef struct tc_serve_stats {

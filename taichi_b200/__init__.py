@@ -25,6 +25,7 @@ TC_FLAG_NO_WIDE = 0x20
 TC_FLAG_NO_WINDOW = 0x40
 TC_FLAG_WINDOW = 0x80
 TC_FLAG_WIDE_BOUNDS = 0x100
+TC_FLAG_WIDE_FIXED = 0x200
 
 _IP = C.POINTER(C.c_int)
 

@@ -127,6 +127,7 @@ struct DevPlan {
                             // every tile is a wide direct tile (the direct kernel), or 4
                             // when every tile is a stream tile (the stream kernel)
     int *err;               // device error word (1: a bounded wait gave up)
+    int wide_rows;          // rows of each wide direct tile (the last may have fewer)
     // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
     const Tile *wtiles;
     int nwtiles;
@@ -162,6 +163,7 @@ struct tc_plan {
     int max_span = 0;
     int stage_rp = 8, stage_cw = 8, grid = 1;
     int *d_err = nullptr;
+    int wide_rows = 0;                   // rows of each wide direct tile
     // window plan (tc_window.cu); nwtiles == 0 when the plan has none
     tc::Tile *d_wtiles = nullptr;
     int nwtiles = 0, wlo = 0, whi = 0, w_rp = 0, w_cw = 0, w_xw = 0, w_stages = 0, w_grid = 0;
@@ -192,6 +194,13 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol,
 // a small matrix still spreads over the GPU.
 void plan_tiles(const int *rowptr, int M, const tc_params &prm, int min_tiles,
                 std::vector<Tile> &tiles, int *nvec, int *nlong);
+// Rows of a wide direct tile: the multiple of 4 that makes two equal tiles
+// per SM (between kDirectRows and kDirectWideRows), so no SM holds twice the
+// rows of another
+// (R-MAT scale 20: 296 tiles of 3,544 rows; 4.99 against 5.20 us per
+// multiply for 256 tiles of 4,096 rows on the same box); kDirectWideRows
+// with TC_FLAG_WIDE_FIXED.
+int wide_tile_rows(int M, const tc_params &prm, int sms);
 // Resident CTAs per SM the lean one-CTA-per-tile kernel is compiled for
 // (40 registers: the stream tiles' words, terms and row pointers fit
 // without spills).

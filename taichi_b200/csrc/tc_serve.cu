@@ -101,6 +101,8 @@ struct tc_server {
     struct Ctx {
         cudaStream_t s = nullptr;
         cudaEvent_t done = nullptr;
+        cudaStream_t s2 = nullptr;          // large requests' own launches, beside the batch launch
+        cudaEvent_t fork = nullptr, join = nullptr;
         float *arena = nullptr;            // device x / y slots (host-vector requests)
         std::vector<uint64_t> reqs;        // tickets of the batch in flight
         bool busy = false;
@@ -199,7 +201,7 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
         }
         if (sv->cfg.solo_bytes > 0 && p->spmv_bytes() >= sv->cfg.solo_bytes) {
             // a large matrix runs its own multiply kernel (the one tc_spmv
-            // launches) after the batch's shared launches, on the same stream
+            // launches) on the context's second stream, beside the batch launch
             solo.push_back(tc::ReqDesc{s.matrix, 0, dx, dy});
             order.emplace_back(tk, 1);
         } else {
@@ -212,13 +214,19 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
         pending.pop_front();
     }
     if (order.empty()) return TC_OK;
+    if (!solo.empty()) {                           // after the x copies
+        TC_CUDA(cudaEventRecord(c.fork, c.s));
+        TC_CUDA(cudaStreamWaitEvent(c.s2, c.fork, 0));
+        for (const tc::ReqDesc &d : solo) TC_CHECK(tc::launch_plan(sv->plans[d.plan], d.x, d.y, c.s2));
+        TC_CUDA(cudaEventRecord(c.join, c.s2));
+    }
     const bool lean = sv->nonlean == 0;
     if (tiles > 0) {
         if (lean) tc::serve_kernel<true><<<tiles, tc::kBlock, 0, c.s>>>(sv->d_plans, args);
         else tc::serve_kernel<false><<<tiles, tc::kBlock, 0, c.s>>>(sv->d_plans, args);
     }
     TC_CUDA(cudaGetLastError());
-    for (const tc::ReqDesc &d : solo) TC_CHECK(tc::launch_plan(sv->plans[d.plan], d.x, d.y, c.s));
+    if (!solo.empty()) TC_CUDA(cudaStreamWaitEvent(c.s, c.join, 0));
     if (!dv) {
         int k[2] = {0, 0};
         for (auto &o : order) {
@@ -328,7 +336,7 @@ void tc_serve_config_default(tc_serve_config *c)
     c->max_plans = 1024;
     c->max_inflight = 2;
     c->max_pending = 1 << 16;
-    c->solo_bytes = 0;
+    c->solo_bytes = 16LL << 20;
 }
 
 tc_status tc_server_create(const tc_serve_config *cfg, tc_server **out)
@@ -363,6 +371,9 @@ tc_status tc_server_create(const tc_serve_config *cfg, tc_server **out)
     for (auto &x : sv->ctx) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x.s2, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x.join, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaMalloc(&x.arena, (size_t)c.arena_bytes);
     }
     if (e != cudaSuccess) {
@@ -650,7 +661,11 @@ tc_status tc_server_destroy(tc_server *sv)
     for (auto &c : sv->ctx) {
         if (c.s) cudaStreamSynchronize(c.s);
         if (c.arena) cudaFree(c.arena);
+        if (c.s2) cudaStreamSynchronize(c.s2);
         if (c.done) cudaEventDestroy(c.done);
+        if (c.fork) cudaEventDestroy(c.fork);
+        if (c.join) cudaEventDestroy(c.join);
+        if (c.s2) cudaStreamDestroy(c.s2);
         if (c.s) cudaStreamDestroy(c.s);
     }
     if (sv->d_plans) cudaFree(sv->d_plans);

@@ -43,6 +43,14 @@ static int kind_of(int lanes)
     return k;
 }
 
+int wide_tile_rows(int M, const tc_params &prm, int sms)
+{
+    if ((prm.flags & TC_FLAG_WIDE_FIXED) || sms <= 0) return kDirectWideRows;
+    // two tiles per SM: every SM holds two CTAs of the same size
+    const long per = ((long)M + 2L * sms - 1) / (2L * sms);
+    return (int)std::min<long>(kDirectWideRows, std::max<long>(kDirectRows, (per + 3) & ~3L));
+}
+
 void plan_tiles(const int *rp, int M, const tc_params &prm, int min_tiles, std::vector<Tile> &tiles,
                 int *nvec, int *nlong)
 {
@@ -59,8 +67,9 @@ void plan_tiles(const int *rp, int M, const tc_params &prm, int min_tiles, std::
         bool short_rows = true;
         for (int i = 0; i < M && short_rows; ++i) short_rows = rp[i + 1] - rp[i] <= kStreamRowMax;
         if (short_rows) {
-            for (int r = 0; r < M; r += kDirectWideRows) {
-                const int n = std::min(kDirectWideRows, M - r);
+            const int R = wide_tile_rows(M, prm, min_tiles / 4);
+            for (int r = 0; r < M; r += R) {
+                const int n = std::min(R, M - r);
                 tiles.push_back(Tile{r, rp[r], rp[r + n] - rp[r], tile_word(n, TILE_DIRECT_WIDE)});
             }
             return;
@@ -219,17 +228,22 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
                                                                      float *__restrict__ y)
 {
     allow_next_grid();
-    // wide tiles are laid out in order, kDirectWideRows rows each, so the
-    // rows are known without waiting for the tile record; only the diagonal
-    // class comes from it
-    const int row0 = blockIdx.x * kDirectWideRows;
+    // wide tiles are laid out in order, p.wide_rows rows each (the last one
+    // may be shorter), so the rows are known without waiting for the tile
+    // record; only the diagonal class comes from it
+    const int row0 = blockIdx.x * p.wide_rows;
+    const int nr = min(p.wide_rows, p.M - row0);
     const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
     if (FULL) {
-        if (threadIdx.x == 0) prefetch_l2(x + row0, kDirectWideRows * sizeof(float));
+        if (threadIdx.x == 0) prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
+        if (4 * (int)threadIdx.x >= nr) {
+            wait_prior_grid(x, y);
+            return;
+        }
         direct_run_full<SIGNED>(p, dc, x, y, row0 + 4 * threadIdx.x);
     } else {
-        if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, kDirectWideRows);
-        direct_run<SIGNED>(p, row0, min(kDirectWideRows, p.M - row0), dc, x, y, true, 4 * threadIdx.x);
+        if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
+        direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
     }
 }
 
@@ -430,9 +444,9 @@ static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const flo
     attr[0].val.programmaticStreamSerializationAllowed = dp.pdl ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const bool full = dp.M % kDirectWideRows == 0 && dp.N >= dp.M &&
+    const bool full = dp.M % 4 == 0 && dp.N >= dp.M &&
                       ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
-    if (dp.per_tile == 3 && full && wb)
+    if (dp.per_tile == 3 && full && wb && dp.wide_rows == kDirectWideRows && dp.M % kDirectWideRows == 0)
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_bounds_kernel<SIGNED>, dp, *wb, x, y));
     else if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, false>, dp, x, y));
@@ -507,6 +521,7 @@ tc::DevPlan tc_plan::dev_plan() const
                : ntiles_stream == ntiles ? 4
                : ntiles_lanes == 0 ? 2 : 1;
     d.err = d_err;
+    d.wide_rows = wide_rows;
     d.wtiles = d_wtiles;
     d.nwtiles = nwtiles;
     d.wlo = wlo;
@@ -567,7 +582,7 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     }
     // the direct kernel finds a wide tile's rows from its index
     for (size_t i = 0; i < tiles.size() && p->ntiles_wide; ++i)
-        if (tiles[i].row0 != (int)i * kDirectWideRows || tile_kind(tiles[i]) != TILE_DIRECT_WIDE)
+        if (tiles[i].row0 != (int)i * tile_nrows(tiles[0]) || tile_kind(tiles[i]) != TILE_DIRECT_WIDE)
             return fail(TC_ERR_FORMAT, "wide tile %d out of order", (int)i);
     for (const Tile &t : tiles) {
         p->ntiles_lanes += tile_kind(t) <= TILE_L32 || tile_kind(t) == TILE_MERGE;
@@ -576,6 +591,7 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     }
     p->ntiles = (int)tiles.size();
     p->nnz_csr = csrRow[M];
+    p->wide_rows = p->ntiles_wide ? tile_nrows(tiles[0]) : kDirectWideRows;
     p->h_wide_nz.clear();
     if (p->ntiles_wide == p->ntiles && p->ntiles > 0 && p->ntiles <= kWideBoundTiles &&
         M % kDirectWideRows == 0 && (p->params.flags & TC_FLAG_WIDE_BOUNDS)) {

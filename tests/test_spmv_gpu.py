@@ -175,7 +175,7 @@ def test_wide_direct_tiles(tc, dev, M):
     N = M + 7
     rp, col = csr_from_lengths(lengths, N, 9)
     assert rp[-1] <= M
-    plan = tc.Plan.from_csr(M, N, rp, col, partition=False)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=tc.TC_FLAG_WIDE_FIXED), partition=False)
     assert plan.info()["ntiles"] == (M + 4095) // 4096              # wide tiles
     check_plan(plan, dict(dense_nnz=0), M, N, rp, col, dev, "wide/M%d" % M)
     x = rng.uniform(-1, 1, N).astype(np.float32)
@@ -441,11 +441,33 @@ def test_wide_bounds_kernel(tc, dev):
     cases_.append(("overfull", M2, rp2, col2))
     x = np.random.default_rng(6).uniform(-1, 1, M2 * 4).astype(np.float32)
     for name, M, rp, col in cases_:
-        plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_WIDE_BOUNDS), partition=False)
+        fixed = tc.TC_FLAG_WIDE_FIXED
+        plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_WIDE_BOUNDS | fixed), partition=False)
         assert plan.info()["ntiles"] == M // 4096
         check_plan(plan, dict(dense_nnz=0), M, M, rp, col, dev, "bounds/" + name)
         y1 = run_spmv(plan, x[:M], M, dev)
         plan.close()
-        plan = tc.Plan.from_csr(M, M, rp, col, partition=False)
+        plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=fixed), partition=False)
         np.testing.assert_array_equal(run_spmv(plan, x[:M], M, dev), y1, err_msg=name)
         plan.close()
+
+
+@pytest.mark.parametrize("M", [1 << 18, 300004, 10001])
+def test_wide_balanced_tiles(tc, dev, M):
+    """Wide tiles sized for two per SM (the default): a whole number of
+    tiles, a short last tile (M a multiple of 4) and an M that is not a
+    multiple of 4 -- against the oracle and bit-identical to 4096-row tiles
+    (TC_FLAG_WIDE_FIXED)."""
+    rng = np.random.default_rng(M)
+    lengths = rng.integers(0, 2, M)
+    lengths[rng.integers(0, M, 30)] = rng.integers(2, 60, 30)
+    rp, col = csr_from_lengths(lengths, M, 10)
+    assert rp[-1] <= M
+    plan = tc.Plan.from_csr(M, M, rp, col, partition=False)
+    check_plan(plan, dict(dense_nnz=0), M, M, rp, col, dev, "balanced/M%d" % M)
+    x = rng.uniform(-1, 1, M).astype(np.float32)
+    y_bal = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_WIDE_FIXED), partition=False)
+    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_bal)
+    plan.close()
