@@ -315,8 +315,7 @@ struct MergeSmem {
 };
 union TileSmem {
     MergeSmem merge;
-    float4 vals4[kStreamNnz / 4 + 2];   // stream tiles: the tile's aligned word window
-    float vals[kStreamNnz + 8];
+    float vals[kStreamNnz + 8 + (kStreamNnz + 8) / 32 + 1];   // stream tiles (skewed, see vslot)
 };
 __device__ __forceinline__ TileSmem &tile_smem()
 {
@@ -394,7 +393,7 @@ __device__ void tile_merge(const DevPlan &p, const Tile &t, const Src &src,
 // never leaves it); each thread turns its kStreamQ int4s per round into
 // kStreamQ * 4 signed x terms, all loads in flight together, and stores them
 // as float4s in shared memory at their window position (entry j of the tile
-// at vals[lead + j]).  Words of the window outside the tile are valid column
+// at slot vslot(lead + j)).  Words of the window outside the tile are valid column
 // words of neighbouring tiles (or the zero padding, column 0), so their
 // gathers stay inside x and their slots are never read.  Then each row's
 // dense-diagonal terms (offset order) and entries (stored order) are added
@@ -425,7 +424,15 @@ __device__ __forceinline__ void stream_words_first(const DevPlan &p, const Tile 
     }
 }
 
-// vals[lead + j] = signed x term of entry j of the tile; ends with a barrier.
+// Shared-memory slot of window entry j of a stream tile: one spare slot per
+// 32 entries, so threads summing rows of equal length L read banks that
+// differ even when L is a multiple of 32 (without the skew, rows of exactly
+// 32 entries put every lane of a warp on one bank: a banded matrix of such
+// rows ran 341 us per multiply against 87 us for rows of 37).
+__device__ __forceinline__ int vslot(int j) { return j + (j >> 5); }
+
+// vals[vslot(lead + j)] = signed x term of entry j of the tile; ends with a
+// barrier.
 template <bool SIGNED>
 __device__ __forceinline__ void stream_gather(const float *__restrict__ x, float *vals, StreamWords &sw)
 {
@@ -451,7 +458,13 @@ __device__ __forceinline__ void stream_gather(const float *__restrict__ x, float
 #pragma unroll
         for (int q = 0; q < kStreamQ; ++q) {
             const int i = base + tid + q * kBlock;
-            if (i < sw.nq) reinterpret_cast<float4 *>(vals)[i] = v[q];
+            if (i < sw.nq) {
+                float *d = vals + vslot(4 * i);      // 4i .. 4i + 3 share one 32-entry group
+                d[0] = v[q].x;
+                d[1] = v[q].y;
+                d[2] = v[q].z;
+                d[3] = v[q].w;
+            }
         }
     }
     __syncthreads();
@@ -507,7 +520,7 @@ __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__rest
         const int rl = tid + k * kBlock;
         if (rl < nr) {
             float acc = diag_tile_row(p, x, dc, row0 + rl);
-            for (int j = rb[k]; j < re[k]; ++j) acc += vals[j];
+            for (int j = rb[k]; j < re[k]; ++j) acc += vals[vslot(j)];
             y[row0 + rl] = acc;
         }
     }
@@ -550,7 +563,7 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
             if (g + u < nr) {
                 acc[u] = diag_tile_row(p, x, dc, row0 + g + u);
                 const int e = g + u + 1 < nr ? b[u + 1] : b[4];
-                for (int j = b[u]; j < e; ++j) acc[u] += vals[j];
+                for (int j = b[u]; j < e; ++j) acc[u] += vals[vslot(j)];
             }
         }
         float *yr = y + row0 + g;
@@ -671,12 +684,33 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
     int c[kDirectW];
 #pragma unroll
     for (int w = 0; w < kDirectW; ++w) c[w] = b[0] + w < e4 ? __ldg(p.cols + b[0] + w) : 0;
+    // a one-shape class with a single dense diagonal (self loops): its column
+    // offset is plan data, read before the wait, so the 4 diagonal loads go
+    // out with the gathers instead of after two dependent plan reads
+    int dcol = 0;
+    bool one = false;
+    if (SIGNED && dc != kDiagNone && dc != kDiagGeneral) {
+        const int2 dr = __ldg(p.shape_dias + dc - 1);
+        if (dr.y - dr.x == 1) {
+            const int4 sh = __ldg(p.shapes + dc - 1);
+            dcol = sh.z - sh.x + __ldg(p.offsets + dr.x);
+            one = true;
+        }
+    }
     wait_prior_grid(x, y);
     float v[kDirectW];
 #pragma unroll
     for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    if (SIGNED) diag_run4(p, x, dc, g, 4, acc);
+    if (SIGNED && one) {
+        float d[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) d[u] = ldx(x + g + u + dcol);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] += d[u];
+    } else if (SIGNED) {
+        diag_run4(p, x, dc, g, 4, acc);
+    }
 #pragma unroll
     for (int w = 0; w < kDirectW; ++w)
 #pragma unroll
