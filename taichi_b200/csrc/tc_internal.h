@@ -128,6 +128,9 @@ struct DevPlan {
                             // when every tile is a stream tile (the stream kernel)
     int *err;               // device error word (1: a bounded wait gave up)
     int wide_rows;          // rows of each wide direct tile (the last may have fewer)
+    // plans whose dense part is one diagonal (one shape, one offset): rows
+    // [d1_lo, d1_hi) add x[r + d1_col] and no other row has a diagonal term
+    int diag1, d1_lo, d1_hi, d1_col;
     // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
     const Tile *wtiles;
     int nwtiles;

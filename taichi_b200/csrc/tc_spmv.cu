@@ -233,7 +233,9 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     // record; only the diagonal class comes from it
     const int row0 = blockIdx.x * p.wide_rows;
     const int nr = min(p.wide_rows, p.M - row0);
-    const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+    // a one-diagonal plan needs no tile record: the parameters say which
+    // rows have the term
+    const int dc = SIGNED && !p.diag1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
     if (FULL) {
         if (threadIdx.x == 0) prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
         if (4 * (int)threadIdx.x >= nr) {
@@ -522,6 +524,16 @@ tc::DevPlan tc_plan::dev_plan() const
                : ntiles_lanes == 0 ? 2 : 1;
     d.err = d_err;
     d.wide_rows = wide_rows;
+    d.diag1 = 0;
+    d.d1_lo = d.d1_hi = d.d1_col = 0;
+    if (dia_shapes == 1 && num_negs == 1 && !h_offsets.empty()) {
+        // the rows where diag_row adds the one term (TaiChi.cu:1014-1023)
+        const int off = h_offsets[0], xs = h_xStart[0], xe = h_xStop[0];
+        d.diag1 = 1;
+        d.d1_lo = std::max(xs + std::max(0, -off), row_start);
+        d.d1_hi = std::min(xe - std::max(0, off), row_stop);
+        d.d1_col = h_yStart[0] - xs + off;
+    }
     d.wtiles = d_wtiles;
     d.nwtiles = nwtiles;
     d.wlo = wlo;

@@ -684,30 +684,30 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
     int c[kDirectW];
 #pragma unroll
     for (int w = 0; w < kDirectW; ++w) c[w] = b[0] + w < e4 ? __ldg(p.cols + b[0] + w) : 0;
-    // a one-shape class with a single dense diagonal (self loops): its column
-    // offset is plan data, read before the wait, so the 4 diagonal loads go
-    // out with the gathers instead of after two dependent plan reads
-    int dcol = 0;
-    bool one = false;
-    if (SIGNED && dc != kDiagNone && dc != kDiagGeneral) {
-        const int2 dr = __ldg(p.shape_dias + dc - 1);
-        if (dr.y - dr.x == 1) {
-            const int4 sh = __ldg(p.shapes + dc - 1);
-            dcol = sh.z - sh.x + __ldg(p.offsets + dr.x);
-            one = true;
-        }
-    }
     wait_prior_grid(x, y);
     float v[kDirectW];
 #pragma unroll
     for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    if (SIGNED && one) {
-        float d[4];
+    if (SIGNED && p.diag1) {
+        // one dense diagonal: which rows have its term comes from the launch
+        // parameters (no plan reads on the chain); the terms and order of
+        // diag_run4
+        const float *xd = x + g + p.d1_col;
+        if (g >= p.d1_lo && g + 4 <= p.d1_hi && (p.d1_col & 3) == 0) {   // x is 16-byte aligned
+            float d[4];
+            asm("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];"
+                : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3]) : "l"(xd));
 #pragma unroll
-        for (int u = 0; u < 4; ++u) d[u] = ldx(x + g + u + dcol);
+            for (int u = 0; u < 4; ++u) acc[u] += d[u];
+        } else {
+            float d[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) acc[u] += d[u];
+            for (int u = 0; u < 4; ++u) d[u] = g + u >= p.d1_lo && g + u < p.d1_hi ? ldx(xd + u) : 0.f;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (g + u >= p.d1_lo && g + u < p.d1_hi) acc[u] += d[u];
+        }
     } else if (SIGNED) {
         diag_run4(p, x, dc, g, 4, acc);
     }

@@ -471,3 +471,23 @@ def test_wide_balanced_tiles(tc, dev, M):
     plan = tc.Plan.from_csr(M, M, rp, col, prm=tc.params(flags=tc.TC_FLAG_WIDE_FIXED), partition=False)
     np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_bal)
     plan.close()
+
+
+@pytest.mark.parametrize("off,keep", [(0, 1.0), (6, 0.98), (-3, 1.0)])
+def test_single_diagonal_wide_plans(tc, dev, off, keep):
+    """Plans whose dense part is one diagonal (one shape, one offset; holes
+    when keep < 1) and whose CSR remainder averages under one entry per row
+    run the wide tiles with the diagonal's rows taken from the launch
+    parameters: against the oracle (format from the reference-pinned oracle
+    partition) and bit-identical to the plan without wide tiles."""
+    M, N, rp, col = matgen.segments(300000, [(0, 300000, off, 0, keep)], noise=60000, seed=5)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    assert fmt["dia_shapes"] == 1 and fmt["num_negs"] == 1, (fmt["dia_shapes"], fmt["num_negs"])
+    plan = tc.Plan.from_format(M, N, fmt)
+    check_plan(plan, fmt, M, N, rp, col, dev, "diag1/off%d" % off)
+    x = np.random.default_rng(2).uniform(-1, 1, N).astype(np.float32)
+    y_wide = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=tc.TC_FLAG_NO_WIDE))
+    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_wide)
+    plan.close()
