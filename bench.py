@@ -528,22 +528,27 @@ def batched_record(args):
 
 
 def highest_passing_rate(serve_at, rates, bisect_steps, limit_ms=2.0):
-    """Sweeps `rates` (increasing) until a rate's p99 reaches limit_ms, then
-    bisects between the last passing and the first failing rate.
-    serve_at(rate) -> stats dict.  Returns (stats of the best passing run or
-    None, list of (rate, stats) of every run)."""
-    runs, best, fail = [], None, None
+    """Sweeps `rates` (increasing) until two rates in a row reach a p99 of
+    limit_ms (one failure alone may be a passing stall of the host, so the
+    sweep goes on), then bisects between the highest passing rate and the
+    first failing rate above it.  serve_at(rate) -> stats dict.  Returns
+    (stats of the best passing run or None, list of (rate, stats) of every
+    run)."""
+    runs, best, fails = [], None, 0
     for rate in rates:
         st = serve_at(rate)
         runs.append((rate, st))
         if st["p99_ms"] < limit_ms:
+            fails = 0
             if best is None or st["spmv_per_s"] > best[1]["spmv_per_s"]:
                 best = (rate, st)
         else:
-            fail = rate
-            break
-    if best is not None and fail is not None and bisect_steps > 0:
-        a, b = best[0], fail
+            fails += 1
+            if fails == 2:
+                break
+    above = [r for r, st in runs if st["p99_ms"] >= limit_ms and best is not None and r > best[0]]
+    if best is not None and above and bisect_steps > 0:
+        a, b = best[0], min(above)
         for _ in range(bisect_steps):
             mid = 0.5 * (a + b)
             st = serve_at(mid)

@@ -131,6 +131,7 @@ struct DevPlan {
     // plans whose dense part is one diagonal (one shape, one offset): rows
     // [d1_lo, d1_hi) add x[r + d1_col] and no other row has a diagonal term
     int diag1, d1_lo, d1_hi, d1_col;
+    int skew;               // stream tiles use skewed shared-memory slots (vslot)
     // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
     const Tile *wtiles;
     int nwtiles;
@@ -167,6 +168,7 @@ struct tc_plan {
     int stage_rp = 8, stage_cw = 8, grid = 1;
     int *d_err = nullptr;
     int wide_rows = 0;                   // rows of each wide direct tile
+    int stream_skew = 0;                 // the plan's usual row length is a multiple of 8
     // window plan (tc_window.cu); nwtiles == 0 when the plan has none
     tc::Tile *d_wtiles = nullptr;
     int nwtiles = 0, wlo = 0, whi = 0, w_rp = 0, w_cw = 0, w_xw = 0, w_stages = 0, w_grid = 0;

@@ -524,6 +524,7 @@ tc::DevPlan tc_plan::dev_plan() const
                : ntiles_lanes == 0 ? 2 : 1;
     d.err = d_err;
     d.wide_rows = wide_rows;
+    d.skew = stream_skew;
     d.diag1 = 0;
     d.d1_lo = d.d1_hi = d.d1_col = 0;
     if (dia_shapes == 1 && num_negs == 1 && !h_offsets.empty()) {
@@ -604,6 +605,17 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
     p->ntiles = (int)tiles.size();
     p->nnz_csr = csrRow[M];
     p->wide_rows = p->ntiles_wide ? tile_nrows(tiles[0]) : kDirectWideRows;
+    {   // the most common length of the rows stream tiles hold: skewed slots
+        // when it is a multiple of 8 (see vslot), sampled rows
+        std::vector<int> h(kStreamRowMax + 1, 0);
+        const int step = std::max(1, M / 65536);
+        for (int r = 0; r < M; r += step) {
+            const int L = csrRow[r + 1] - csrRow[r];
+            if (L <= kStreamRowMax) ++h[L];
+        }
+        const int mode = (int)(std::max_element(h.begin() + 1, h.end()) - h.begin());
+        p->stream_skew = h[mode] > 0 && mode % 8 == 0;
+    }
     p->h_wide_nz.clear();
     if (p->ntiles_wide == p->ntiles && p->ntiles > 0 && p->ntiles <= kWideBoundTiles &&
         M % kDirectWideRows == 0 && (p->params.flags & TC_FLAG_WIDE_BOUNDS)) {

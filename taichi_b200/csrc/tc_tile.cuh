@@ -315,7 +315,8 @@ struct MergeSmem {
 };
 union TileSmem {
     MergeSmem merge;
-    float vals[kStreamNnz + 8 + (kStreamNnz + 8) / 32 + 1];   // stream tiles (skewed, see vslot)
+    float4 vals4[(kStreamNnz + 8 + (kStreamNnz + 8) / 32 + 4) / 4];   // alignment of the stream slots
+    float vals[kStreamNnz + 8 + (kStreamNnz + 8) / 32 + 1];   // stream tiles (see vslot)
 };
 __device__ __forceinline__ TileSmem &tile_smem()
 {
@@ -424,17 +425,19 @@ __device__ __forceinline__ void stream_words_first(const DevPlan &p, const Tile 
     }
 }
 
-// Shared-memory slot of window entry j of a stream tile: one spare slot per
-// 32 entries, so threads summing rows of equal length L read banks that
-// differ even when L is a multiple of 32 (without the skew, rows of exactly
-// 32 entries put every lane of a warp on one bank: a banded matrix of such
-// rows ran 341 us per multiply against 87 us for rows of 37).
+// Shared-memory slot of window entry j of a stream tile of a plan whose
+// rows mostly have a length that is a multiple of 8 (DevPlan::skew): one
+// spare slot per 32 entries, so threads summing rows of equal length L read
+// banks that differ (without the skew, rows of exactly 32 entries put every
+// lane of a warp on one bank: a banded matrix of such rows ran 341 us per
+// multiply against 99 us with it).  Other plans keep slot j (float4 stores,
+// no index arithmetic: the skew cost the 9-point mesh 4 %).
 __device__ __forceinline__ int vslot(int j) { return j + (j >> 5); }
 
-// vals[vslot(lead + j)] = signed x term of entry j of the tile; ends with a
+// vals[slot(lead + j)] = signed x term of entry j of the tile; ends with a
 // barrier.
 template <bool SIGNED>
-__device__ __forceinline__ void stream_gather(const float *__restrict__ x, float *vals, StreamWords &sw)
+__device__ __forceinline__ void stream_gather(const float *__restrict__ x, float *vals, StreamWords &sw, bool skew)
 {
     const int tid = threadIdx.x;
     for (int base = 0; base < sw.nq; base += kStreamQ * kBlock) {
@@ -459,11 +462,15 @@ __device__ __forceinline__ void stream_gather(const float *__restrict__ x, float
         for (int q = 0; q < kStreamQ; ++q) {
             const int i = base + tid + q * kBlock;
             if (i < sw.nq) {
-                float *d = vals + vslot(4 * i);      // 4i .. 4i + 3 share one 32-entry group
-                d[0] = v[q].x;
-                d[1] = v[q].y;
-                d[2] = v[q].z;
-                d[3] = v[q].w;
+                if (skew) {
+                    float *d = vals + vslot(4 * i);  // 4i .. 4i + 3 share one 32-entry group
+                    d[0] = v[q].x;
+                    d[1] = v[q].y;
+                    d[2] = v[q].z;
+                    d[3] = v[q].w;
+                } else {
+                    reinterpret_cast<float4 *>(vals)[i] = v[q];
+                }
             }
         }
     }
@@ -511,7 +518,7 @@ __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__rest
         re[k] = ok ? __ldg(p.rowptr + row0 + rl + 1) - base : 0;
     }
     if (wait) wait_prior_grid(x, y);
-    stream_gather<SIGNED>(x, vals, sw);
+    stream_gather<SIGNED>(x, vals, sw, p.skew);
     // (Loading the rows' diagonal terms while the gathers are in flight
     // measured slower on the mesh: into registers 69.5 against 65.6 us; as
     // the tile's x segment staged in shared memory 58.3 against 52.5 us.)
@@ -520,7 +527,11 @@ __device__ void tile_stream(const DevPlan &p, const Tile &t, const float *__rest
         const int rl = tid + k * kBlock;
         if (rl < nr) {
             float acc = diag_tile_row(p, x, dc, row0 + rl);
-            for (int j = rb[k]; j < re[k]; ++j) acc += vals[vslot(j)];
+            if (p.skew) {
+                for (int j = rb[k]; j < re[k]; ++j) acc += vals[vslot(j)];
+            } else {
+                for (int j = rb[k]; j < re[k]; ++j) acc += vals[j];
+            }
             y[row0 + rl] = acc;
         }
     }
@@ -550,7 +561,7 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
         rp4[k] = ok ? __ldg(p.rowptr + row0 + min(g + 4, nr)) : 0;
     }
     if (wait) wait_prior_grid(x, y);
-    stream_gather<SIGNED>(x, vals, sw);
+    stream_gather<SIGNED>(x, vals, sw, p.skew);
 #pragma unroll
     for (int k = 0; k < GQ; ++k) {
         const int g = 4 * (tid + k * kBlock);
@@ -563,7 +574,11 @@ __device__ void tile_stream4(const DevPlan &p, const Tile &t, const float *__res
             if (g + u < nr) {
                 acc[u] = diag_tile_row(p, x, dc, row0 + g + u);
                 const int e = g + u + 1 < nr ? b[u + 1] : b[4];
-                for (int j = b[u]; j < e; ++j) acc[u] += vals[vslot(j)];
+                if (p.skew) {
+                    for (int j = b[u]; j < e; ++j) acc[u] += vals[vslot(j)];
+                } else {
+                    for (int j = b[u]; j < e; ++j) acc[u] += vals[j];
+                }
             }
         }
         float *yr = y + row0 + g;

@@ -41,8 +41,9 @@ def test_reference_arm_other_ranks_idle():
 def test_highest_passing_rate():
     """The served form's rate search against a fake server whose p99 grows
     with the rate (2 ms at 2,000 requests/s) and which serves every rate in
-    full: the sweep stops at the first failing rate and the bisection closes
-    in on 2,000 from below."""
+    full: the sweep stops after two failing rates in a row and the bisection
+    closes in on 2,000 from below; a lone failing rate (a stall) does not end
+    the sweep."""
     sys.path.insert(0, ROOT)
     import bench
     calls = []
@@ -51,14 +52,17 @@ def test_highest_passing_rate():
         calls.append(rate)
         return {"p99_ms": rate / 1000.0, "spmv_per_s": rate}
 
-    best, runs = bench.highest_passing_rate(serve_at, [500.0, 1000.0, 4000.0, 8000.0], 6)
-    assert calls[:3] == [500.0, 1000.0, 4000.0] and len(calls) == 3 + 6
+    best, runs = bench.highest_passing_rate(serve_at, [500.0, 1000.0, 4000.0, 8000.0, 9000.0], 6)
+    assert calls[:4] == [500.0, 1000.0, 4000.0, 8000.0] and len(calls) == 4 + 6
     assert 2000.0 - 3000.0 / 64 <= best["spmv_per_s"] < 2000.0
     assert len(runs) == len(calls)
+    # a stall at 1,000 only: the sweep goes on to 1,500
+    stall = lambda r: {"p99_ms": 5.0 if r == 1000.0 else r / 1000.0, "spmv_per_s": r}
+    best, runs = bench.highest_passing_rate(stall, [500.0, 1000.0, 1500.0, 2500.0, 3000.0], 0)
+    assert best["spmv_per_s"] == 1500.0
     # nothing passes: no best run, and no bisection
-    calls.clear()
-    best, runs = bench.highest_passing_rate(lambda r: {"p99_ms": 5.0, "spmv_per_s": r}, [100.0, 200.0], 4)
-    assert best is None and len(runs) == 1
+    best, runs = bench.highest_passing_rate(lambda r: {"p99_ms": 5.0, "spmv_per_s": r}, [100.0, 200.0, 300.0], 4)
+    assert best is None and len(runs) == 2
     # everything passes: the highest rate, no bisection
     best, runs = bench.highest_passing_rate(lambda r: {"p99_ms": 0.1, "spmv_per_s": r}, [1.0, 2.0, 3.0], 4)
     assert best["spmv_per_s"] == 3.0 and len(runs) == 3

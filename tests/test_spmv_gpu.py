@@ -491,3 +491,21 @@ def test_single_diagonal_wide_plans(tc, dev, off, keep):
     plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=tc.TC_FLAG_NO_WIDE))
     np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_wide)
     plan.close()
+
+
+@pytest.mark.parametrize("k,r", [(12, 7), (11, 9), (15, 8)])
+def test_stream_rows_multiple_of_8(tc, dev, k, r):
+    """Banded rows of 32 entries (2k + 1 + r = 32; the plan's stream tiles
+    then use skewed shared-memory slots) and of 39 entries (plain slots):
+    against the oracle and bit-identical to one-lane tiles (TILE_L1, the
+    same terms in the same order)."""
+    n = 60000
+    rp, col = tc.gen_banded(n, k, r, seed=3)
+    plan = tc.Plan.from_csr(n, n, rp, col, partition=False)
+    check_plan(plan, dict(dense_nnz=0), n, n, rp, col, dev, "band k%d r%d" % (k, r))
+    x = np.random.default_rng(1).uniform(-1, 1, n).astype(np.float32)
+    y = run_spmv(plan, x, n, dev)
+    plan.close()
+    plan = tc.Plan.from_csr(n, n, rp, col, prm=tc.params(tile_mode=1, max_lanes=1), partition=False)
+    np.testing.assert_array_equal(run_spmv(plan, x, n, dev), y)
+    plan.close()
