@@ -184,6 +184,7 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
     int64_t used = 0;
     std::vector<std::pair<uint64_t, int>> order;    // ticket, 0: shared launch, 1: its own
     std::vector<tc::ReqDesc> solo;
+    c.reqs.clear();                                 // every request taken, so a failure can fail them
     while (!pending.empty() && (int)order.size() < sv->cfg.max_batch) {
         const uint64_t tk = pending.front();
         tc_server::Slot &s = sv->slots[tk & (sv->ring - 1)];
@@ -211,6 +212,7 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
             order.emplace_back(tk, 0);
         }
         s.state.store(tc::kRunning, std::memory_order_relaxed);
+        c.reqs.push_back(tk);
         pending.pop_front();
     }
     if (order.empty()) return TC_OK;
@@ -237,8 +239,6 @@ tc_status launch_batch(tc_server *sv, tc_server::Ctx &c, std::deque<uint64_t> &p
         }
     }
     TC_CUDA(cudaEventRecord(c.done, c.s));
-    c.reqs.clear();
-    for (auto &o : order) c.reqs.push_back(o.first);
     c.busy = true;
     *taken = (int)order.size();
     return TC_OK;
@@ -259,6 +259,7 @@ void dispatcher(tc_server *sv, int device)
             if (q == cudaErrorNotReady) continue;
             const double t = tc::now_s();
             if (q != cudaSuccess) {
+                std::lock_guard<std::mutex> lk(sv->st_mu);
                 sv->worker_error = cudaGetErrorString(q);
                 sv->worker_status.store(TC_ERR_CUDA);
             }
@@ -282,12 +283,15 @@ void dispatcher(tc_server *sv, int device)
             const double tl = tc::now_s();
             const tc_status st = launch_batch(sv, *fc, pending, &taken);
             fc->t_launch = tl;
-            if (st != TC_OK) {
-                sv->worker_error = tc_last_error();
+            if (st != TC_OK) {                           // the requests it took fail
+                {
+                    std::lock_guard<std::mutex> lk(sv->st_mu);
+                    sv->worker_error = tc_last_error();
+                }
                 sv->worker_status.store(st);
-                fc->busy = false;
-                for (uint64_t tk : fc->reqs) pending.push_front(tk);
-                fc->reqs.clear();
+                cudaStreamSynchronize(fc->s);                // nothing of it stays in flight
+                cudaStreamSynchronize(fc->s2);
+                complete_ctx(sv, *fc, tc::now_s(), false);
                 break;
             }
             if (taken == 0) break;                      // (cannot happen: one request always fits)
@@ -522,8 +526,16 @@ tc_status tc_server_poll(tc_server *sv, uint64_t ticket, int *done)
         *done = 1;
         return TC_OK;
     }
-    if (st == tc::kFailed) return fail((tc_status)sv->worker_status.load(), "request %llu failed: %s",
-                                       (unsigned long long)ticket, sv->worker_error.c_str());
+    if (st == tc::kFailed) {
+        std::string why;
+        {
+            std::lock_guard<std::mutex> lk(sv->st_mu);
+            why = sv->worker_error;
+        }
+        const int ws = sv->worker_status.load();
+        return fail(ws != TC_OK ? (tc_status)ws : TC_ERR_CUDA, "request %llu failed: %s",
+                    (unsigned long long)ticket, why.c_str());
+    }
     *done = st == tc::kDone;
     return TC_OK;
 }
@@ -584,7 +596,7 @@ tc_status tc_server_stop(tc_server *sv)
     if (sv->worker.joinable()) sv->worker.join();
     sv->running.store(false);
     const int st = sv->worker_status.load();
-    return st == TC_OK ? TC_OK : fail((tc_status)st, "dispatcher: %s", sv->worker_error.c_str());
+    return st == TC_OK ? TC_OK : fail((tc_status)st, "dispatcher: %s", sv->worker_error.c_str());   // thread joined
 }
 
 tc_status tc_server_run(tc_server *sv, int nreq, const double *arrival_s, const int *matrix,
