@@ -212,6 +212,10 @@ def run_ours(args, rank, world, local_rank):
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_FIXED
     if args.wide_bounds:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_BOUNDS
+    for on, f in ((args.rows, tc.TC_FLAG_ROWS), (args.no_rows, tc.TC_FLAG_NO_ROWS),
+                  (args.rows_pair, tc.TC_FLAG_ROWS_PAIR), (args.no_prefetch, tc.TC_FLAG_NO_PREFETCH)):
+        if on:
+            over["flags"] = over.get("flags", 0) | f
     if args.tile_nnz is not None:
         over["tile_nnz"] = args.tile_nnz
     if args.ctas_per_sm is not None:
@@ -247,31 +251,52 @@ def run_ours(args, rank, world, local_rank):
 
     # The timed multiplies are captured in a CUDA graph and replayed on the
     # device back to back.  Up to 8192 steps: one graph of LEAD untimed
-    # multiplies, an event, exactly --steps multiplies, an event (the events
-    # are graph nodes, so neither the host's graph submission nor the graph's
-    # start-up falls inside the timed span).  More steps: a graph of G
-    # multiplies (G the largest divisor of steps up to 4096) replayed
-    # steps / G times between two stream events, after one untimed replay
-    # that keeps the device busy while the host submits the timed ones.
+    # multiplies, exactly --steps timed ones and LEAD untimed ones.  The two
+    # timing events are graph nodes on a side branch: each is recorded when
+    # the multiply before it has completed, without holding back the next
+    # multiply, which starts under programmatic dependent launch while its
+    # predecessor drains.  The span runs from the completion of the last
+    # multiply before the timed ones to the completion of the last timed
+    # one -- exactly --steps multiplies in steady state, with neither the
+    # host's graph submission nor the graph's start-up in it.  (Events on
+    # the chain itself would make the first timed multiply wait for its
+    # predecessor to finish: that figure is reported beside it as
+    # `chain_bracket_gbs`.)  More steps: a graph of G multiplies (G the
+    # largest divisor of steps up to 4096) replayed steps / G times between
+    # two stream events, after one untimed replay that keeps the device busy
+    # while the host submits the timed ones.
     LEAD = 16
     in_graph = args.steps <= 8192
     G = args.steps if in_graph else graph_len(args.steps)
     reps = args.steps // G
     ev0 = torch.cuda.Event(enable_timing=True, external=in_graph)
     ev1 = torch.cuda.Event(enable_timing=True, external=in_graph)
+    side = torch.cuda.Stream(device=dev)
 
     def spmv_i(i):
         plans[i % ncopy].spmv(xs[i % ncopy], ys[i % ncopy], stream=torch.cuda.current_stream())
+
+    def mark(ev):
+        """Records ev on a side branch after everything captured so far."""
+        f = torch.cuda.Event()
+        f.record(stream)
+        side.wait_event(f)
+        ev.record(side)
 
     g_main = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g_main, stream=stream):
         if in_graph:
             for i in range(LEAD):
                 spmv_i(i)
-            ev0.record()
+            mark(ev0)
             for i in range(args.steps):
                 spmv_i(LEAD + i)
-            ev1.record()
+            mark(ev1)
+            for i in range(LEAD):
+                spmv_i(LEAD + args.steps + i)
+            j = torch.cuda.Event()
+            j.record(side)
+            stream.wait_event(j)
         else:
             for i in range(G):
                 spmv_i(i)
@@ -297,6 +322,25 @@ def run_ours(args, rank, world, local_rank):
     replicas.barrier(world)
     ms = ev0.elapsed_time(ev1)
     cl = clocks.stop()
+    chain_ms = None
+    if in_graph:                            # context: the events on the chain itself
+        c0 = torch.cuda.Event(enable_timing=True, external=True)
+        c1 = torch.cuda.Event(enable_timing=True, external=True)
+        g_chain = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g_chain, stream=stream):
+            for i in range(LEAD):
+                spmv_i(i)
+            c0.record()
+            for i in range(args.steps):
+                spmv_i(LEAD + i)
+            c1.record()
+        with torch.cuda.stream(stream):
+            g_chain.replay()
+            torch.cuda.synchronize()
+            g_chain.replay()
+        torch.cuda.synchronize()
+        chain_ms = c0.elapsed_time(c1)
+        del g_chain
     ms = replicas.max_over_ranks(ms, world, device=dev)    # the slowest replica bounds the job
     ms_step = ms / args.steps
     gbs = bytes_per / (ms_step * 1e-3) / 1e9 * world
@@ -369,17 +413,21 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": args.workload + "_plain_hybrid_spmv", "M": M, "N": N,
                        "nnz": int(rp[M]), "partition": partition,
                        "dia_shapes": info["dia_shapes"], "num_negs": info["num_negs"],
-                       "nnz_csr": info["nnz_csr"], "tiles": info["ntiles"], "tile_mode": prm.tile_mode, "tile_rows": prm.tile_rows,
+                       "nnz_csr": info["nnz_csr"], "tiles": info["ntiles"], "kernel": tc.KERNEL_NAMES.get(info["kernel"]), "tile_mode": prm.tile_mode, "tile_rows": prm.tile_rows,
                        "tile_nnz": prm.tile_nnz, "flags": prm.flags,
                        "bytes_per_spmv": bytes_per, "format_build_s": round(build_s, 3),
                        "partition_ms": info["partition_ms"],
-                       "timing": ("one CUDA graph: %d untimed SpMVs, event, %d timed SpMVs, event "
-                                  "(events are graph nodes)" % (LEAD, args.steps) if in_graph else
+                       "timing": ("one CUDA graph: %d untimed SpMVs, %d timed, %d untimed; events are "
+                                  "graph nodes on a side branch after the last untimed and the last timed "
+                                  "SpMV (steady state, completion to completion)" % (LEAD, args.steps, LEAD)
+                                  if in_graph else
                                   "%d replays of a %d-SpMV graph after an untimed replay, stream events"
                                   % (reps, G)),
                        "l2": "rotating %d resident copies (%.0f MB) > 2x L2" % (
                            ncopy, ncopy * bytes_per / 1e6),
                        "warm_l2_gbs": round(bytes_per / (warm_ms * 1e-3) / 1e9, 1),
+                       "chain_bracket_gbs": (round(bytes_per * args.steps / (chain_ms * 1e-3) / 1e9, 1)
+                                             if chain_ms else None),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": {"bound": "hbm", "achieved": round(gbs / world, 2), "peak": peak,
                          "unit": "GB/s", "frac": round(gbs / world / peak, 4),
@@ -665,6 +713,11 @@ def main():
                     help="wide plans: tiles of 4096 rows instead of two equal tiles per SM")
     ap.add_argument("--wide-bounds", action="store_true",
                     help="wide plans: tile word ranges in the launch parameters, words staged in shared memory")
+    ap.add_argument("--rows", action="store_true", help="stream plans: the rows kernel whatever the row lengths")
+    ap.add_argument("--no-rows", action="store_true", help="stream plans: never the rows kernel")
+    ap.add_argument("--rows-pair", action="store_true", help="the rows kernel: two rows per thread")
+    ap.add_argument("--no-prefetch", action="store_true",
+                    help="stream / rows kernels: no L2 prefetch of the operands a wave ahead")
     ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")
     ap.add_argument("--serve-max-batch", type=int, default=64, help="served form: most requests per launch")
     ap.add_argument("--serve-inflight", type=int, default=2, help="served form: batches on the GPU at once")

@@ -85,6 +85,17 @@ typedef struct tc_params {
                                      slower on R-MAT scale 20)              */
 #define TC_FLAG_WIDE_FIXED   0x200 /* wide plans: tiles of 4096 rows
                                      instead of two equal tiles per SM     */
+#define TC_FLAG_ROWS         0x400 /* plans of stream tiles only: run the
+                                     rows kernel (one row per thread, words
+                                     straight from global memory) whatever
+                                     the rows' mean length                  */
+#define TC_FLAG_NO_ROWS      0x800 /* plans of stream tiles only: never run
+                                     the rows kernel                        */
+#define TC_FLAG_ROWS_PAIR    0x1000 /* the rows kernel runs two rows per
+                                     thread (half the CTAs)                 */
+#define TC_FLAG_NO_PREFETCH  0x2000 /* stream and rows kernels: no L2
+                                     prefetch of the operands of the CTA a
+                                     wave ahead                             */
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */
@@ -140,7 +151,17 @@ typedef struct tc_plan_info {
     int nwtiles;              /* window tiles (0: the plan has no window plan) */
     int window_lo, window_hi; /* x window of rows [r0, r0+n):
                                  [r0 + window_lo, r0 + n + window_hi)          */
+    int kernel;               /* the multiply's kernel: TC_KERNEL_*            */
 } tc_plan_info;
+
+/* tc_plan_info.kernel */
+#define TC_KERNEL_TILES   0   /* persistent grid over staged tiles (tile_mode 0 / 1) */
+#define TC_KERNEL_GRID    1   /* one CTA per tile, every tile kind              */
+#define TC_KERNEL_LEAN    2   /* one CTA per tile: stream, direct and long tiles */
+#define TC_KERNEL_WIDE    3   /* wide direct tiles, one 1024-thread CTA each     */
+#define TC_KERNEL_STREAM  4   /* stream tiles only                              */
+#define TC_KERNEL_ROWS    5   /* one row per thread, no tiles                   */
+#define TC_KERNEL_WINDOW  6   /* window tiles (x staged per tile)               */
 
 TC_API tc_status tc_plan_info_get(const tc_plan *plan, tc_plan_info *info);
 

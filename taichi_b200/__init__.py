@@ -26,6 +26,10 @@ TC_FLAG_NO_WINDOW = 0x40
 TC_FLAG_WINDOW = 0x80
 TC_FLAG_WIDE_BOUNDS = 0x100
 TC_FLAG_WIDE_FIXED = 0x200
+TC_FLAG_ROWS = 0x400
+TC_FLAG_NO_ROWS = 0x800
+TC_FLAG_ROWS_PAIR = 0x1000
+TC_FLAG_NO_PREFETCH = 0x2000
 
 _IP = C.POINTER(C.c_int)
 
@@ -57,7 +61,10 @@ class PlanInfo(C.Structure):
                 ("nnz_csr", C.c_int64), ("ntiles", C.c_int), ("ntiles_vector", C.c_int),
                 ("ntiles_long", C.c_int), ("device_bytes", C.c_int64), ("spmv_bytes", C.c_int64),
                 ("partition_ms", C.c_double), ("num_contours", C.c_int), ("nwtiles", C.c_int),
-                ("window_lo", C.c_int), ("window_hi", C.c_int)]
+                ("window_lo", C.c_int), ("window_hi", C.c_int), ("kernel", C.c_int)]
+
+
+KERNEL_NAMES = {0: "tiles", 1: "grid", 2: "lean", 3: "wide", 4: "stream", 5: "rows", 6: "window"}
 
 
 # extern "C" symbols declared in include/taichi_b200.h (checked by the tests)

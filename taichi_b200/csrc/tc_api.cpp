@@ -197,6 +197,12 @@ tc_status tc_plan_info_get(const tc_plan *p, tc_plan_info *i)
     i->nwtiles = p->nwtiles;
     i->window_lo = p->wlo;
     i->window_hi = p->whi;
+    {
+        const tc::DevPlan d = p->dev_plan();
+        i->kernel = d.nwtiles > 0 ? TC_KERNEL_WINDOW : d.per_tile == 4 && d.rows ? TC_KERNEL_ROWS
+                  : d.per_tile == 0 ? TC_KERNEL_TILES : d.per_tile == 1 ? TC_KERNEL_GRID
+                  : d.per_tile == 2 ? TC_KERNEL_LEAN : d.per_tile == 3 ? TC_KERNEL_WIDE : TC_KERNEL_STREAM;
+    }
     return TC_OK;
 }
 

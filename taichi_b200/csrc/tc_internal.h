@@ -88,6 +88,10 @@ constexpr int kStreamRowMax = 128;    // longer rows leave stream tiles for lane
 constexpr int kStream4Rows = 1024;    // most rows of a TILE_STREAM4 tile (a run of 4 per thread)
 constexpr int kDirectRows = 1024;     // most rows of a direct tile (TILE_DIRECT4)
 constexpr int kDirectWideBlock = 1024; // threads of the direct kernel's CTAs
+constexpr int kPlanDiags = 8;         // dense diagonals a plan can carry in its launch parameters
+constexpr int kRowsW = 8;             // CSR words of a row the rows kernel loads together
+constexpr int kRowsMeanMax = 12;      // rows kernel by default: mean CSR words per row at most this
+constexpr bool kRowsByDefault = false;
 constexpr int kDirectWideRows = 4 * kDirectWideBlock;   // most rows of a TILE_DIRECT_WIDE tile
 // A wide plan of at most kWideBoundTiles whole tiles passes each tile's
 // first CSR word in the launch parameters (WideBounds), so a CTA loads its
@@ -128,9 +132,16 @@ struct DevPlan {
                             // when every tile is a stream tile (the stream kernel)
     int *err;               // device error word (1: a bounded wait gave up)
     int wide_rows;          // rows of each wide direct tile (the last may have fewer)
-    // plans whose dense part is one diagonal (one shape, one offset): rows
-    // [d1_lo, d1_hi) add x[r + d1_col] and no other row has a diagonal term
-    int diag1, d1_lo, d1_hi, d1_col;
+    // plans whose dense part is one shape of at most kPlanDiags offsets
+    // (dn of them, in offset order): offset i adds x[r + d_col[i]] to the rows
+    // r of [d_lo[i], d_hi[i]) and no other row has a diagonal term.  dn = 0:
+    // no dense part, or more than one shape / more offsets (dgen = 1: the
+    // per-row shape search, diag_row)
+    int dn, dgen;
+    int d_lo[kPlanDiags], d_hi[kPlanDiags], d_col[kPlanDiags];
+    int rows;               // stream plan run by the rows kernel (one row per thread)
+    int rows_pair;          // the rows kernel's CTAs run two strips of rows
+    int ahead;              // stream / rows kernels: CTA b prefetches the operands of CTA b + ahead
     int skew;               // stream tiles use skewed shared-memory slots (vslot)
     // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
     const Tile *wtiles;
@@ -216,6 +227,9 @@ constexpr int kLeanMinBlocks = 6, kLeanMinBlocksSigned = 6;
 // µs); a single wave loses from the thinner threads (n = 65,536 random
 // matrix: 5.6 -> 6.7 µs), so a plan takes it only above one wave.
 constexpr int kStreamManyMinBlocks = 8;
+// The rows kernel: 8 CTAs per SM (32 registers) with one strip of rows per
+// CTA, 4 with two.
+constexpr int kRowsMinBlocks = 8;
 // The same for the batch and served kernels, which read the plan descriptor
 // from memory instead of the parameter bank (48 registers).
 constexpr int kItemMinBlocks = 5;

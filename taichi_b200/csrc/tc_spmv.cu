@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     const int nr = min(p.wide_rows, p.M - row0);
     // a one-diagonal plan needs no tile record: the parameters say which
     // rows have the term
-    const int dc = SIGNED && !p.diag1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+    const int dc = SIGNED && p.dn != 1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
     if (FULL) {
         if (threadIdx.x == 0) prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
         if (4 * (int)threadIdx.x >= nr) {
@@ -246,6 +246,94 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     } else {
         if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
         direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
+    }
+}
+
+// The multiply of a stream plan of short rows, one row per thread, read
+// straight from global memory: no tile records, shared memory or barriers.
+// A CTA runs RPT strips of kBlock consecutive rows (coalesced row pointers
+// and y stores).  Each thread loads its row's first kRowsW words together
+// (immutable plan data, before griddepcontrol.wait), then their gathers and
+// its dense-diagonal terms together, and adds the diagonal terms (offset
+// order), then the words (stored order), then any further words four at a
+// time: the terms and order of tile_rows_seq, so y is bit-identical to the
+// stream tiles'.  Consecutive lanes hold consecutive rows, so a warp's load
+// of word w of its 32 rows touches the few cache lines holding those rows,
+// and its later words hit L1.  Against the stream tiles it spends no
+// instructions on parking terms in shared memory and no barrier waits.
+template <bool SIGNED, int RPT>
+__global__ void __launch_bounds__(kBlock, RPT == 1 ? kRowsMinBlocks : kRowsMinBlocks / 2)
+    spmv_rows_kernel(DevPlan p, const float *__restrict__ x, float *__restrict__ y)
+{
+    allow_next_grid();
+    const int r0 = blockIdx.x * (kBlock * RPT) + threadIdx.x;
+    // thread 0 also brings into L2 the operands of the strip a wave later
+    const bool ahead = threadIdx.x == 0 && blockIdx.x + p.ahead < gridDim.x;
+    int za = 0, zb = 0;
+    if (threadIdx.x == 0) prefetch_x_window(x, p.N, r0, kBlock * RPT);
+    int b[RPT], e[RPT], c[RPT][kRowsW];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        const int r = r0 + k * kBlock;
+        b[k] = r < p.M ? __ldg(p.rowptr + r) : 0;
+        e[k] = r < p.M ? __ldg(p.rowptr + r + 1) : 0;
+    }
+    if (ahead) {
+        const int ra = (blockIdx.x + p.ahead) * (kBlock * RPT);
+        za = __ldg(p.rowptr + ra);
+        zb = __ldg(p.rowptr + min(ra + kBlock * RPT, p.M));
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+#pragma unroll
+        for (int w = 0; w < kRowsW; ++w) c[k][w] = b[k] + w < e[k] ? __ldg(p.cols + b[k] + w) : 0;
+    if (ahead) {
+        const int ra = (blockIdx.x + p.ahead) * (kBlock * RPT);
+        prefetch_rows_ahead(p, ra, min(ra + kBlock * RPT, p.M), za, zb);
+    }
+    wait_prior_grid(x, y);
+    float v[RPT][kRowsW];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+#pragma unroll
+        for (int w = 0; w < kRowsW; ++w) v[k][w] = b[k] + w < e[k] ? gather<SIGNED>(x, c[k][w]) : 0.f;
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        const int r = r0 + k * kBlock;
+        float acc = 0.f;
+        if (SIGNED && p.dgen) {
+            acc = diag_row(p, x, r);
+        } else if (SIGNED) {
+#pragma unroll 1
+            for (int i = 0; i < p.dn; i += 4) {
+                float d[4];
+                bool in[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    in[u] = i + u < p.dn && r >= p.d_lo[i + u] && r < p.d_hi[i + u];
+                    d[u] = in[u] ? ldx(x + r + p.d_col[i + u]) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (in[u]) acc += d[u];
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < kRowsW; ++w)
+            if (b[k] + w < e[k]) acc += v[k][w];
+#pragma unroll 1
+        for (int j = b[k] + kRowsW; j < e[k]; j += 4) {            // longer rows
+            int cc[4];
+            float vv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cc[u] = j + u < e[k] ? __ldg(p.cols + j + u) : 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) vv[u] = j + u < e[k] ? gather<SIGNED>(x, cc[u]) : 0.f;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (j + u < e[k]) acc += vv[u];
+        }
+        if (r < p.M) y[r] = acc;
     }
 }
 
@@ -305,7 +393,13 @@ __global__ void __launch_bounds__(kBlock, MANY ? kStreamManyMinBlocks
 {
     allow_next_grid();
     const Tile t = p.tiles[blockIdx.x];
-    if (threadIdx.x == 0) prefetch_x_window(x, p.N, t.row0, tile_nrows(t));
+    if (threadIdx.x == 0) {
+        prefetch_x_window(x, p.N, t.row0, tile_nrows(t));
+        if (MANY && blockIdx.x + p.ahead < p.ntiles) {   // the tile a wave later
+            const Tile a = p.tiles[blockIdx.x + p.ahead];
+            prefetch_rows_ahead(p, a.row0, a.row0 + tile_nrows(a), a.nz0, a.nz0 + a.nnz);
+        }
+    }
     tile_stream<SIGNED>(p, t, x, y, true);
 }
 
@@ -452,6 +546,12 @@ static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const flo
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_bounds_kernel<SIGNED>, dp, *wb, x, y));
     else if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, false>, dp, x, y));
+    else if (dp.per_tile == 4 && dp.rows) {
+        const bool pair = (dp.rows_pair != 0);
+        cfg.gridDim = dim3((unsigned)((dp.M + kBlock * (pair ? 2 : 1) - 1) / (kBlock * (pair ? 2 : 1))));
+        if (pair) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 2>, dp, x, y));
+        else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 1>, dp, x, y));
+    }
     else if (dp.per_tile == 4 && dp.ntiles > kLeanMinBlocks * num_sms())
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_stream_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile == 4) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_stream_kernel<SIGNED, false>, dp, x, y));
@@ -525,16 +625,32 @@ tc::DevPlan tc_plan::dev_plan() const
     d.err = d_err;
     d.wide_rows = wide_rows;
     d.skew = stream_skew;
-    d.diag1 = 0;
-    d.d1_lo = d.d1_hi = d.d1_col = 0;
-    if (dia_shapes == 1 && num_negs == 1 && !h_offsets.empty()) {
-        // the rows where diag_row adds the one term (TaiChi.cu:1014-1023)
-        const int off = h_offsets[0], xs = h_xStart[0], xe = h_xStop[0];
-        d.diag1 = 1;
-        d.d1_lo = std::max(xs + std::max(0, -off), row_start);
-        d.d1_hi = std::min(xe - std::max(0, off), row_stop);
-        d.d1_col = h_yStart[0] - xs + off;
+    d.dn = 0;
+    d.dgen = 0;
+    if (dia_shapes == 1 && num_negs <= tc::kPlanDiags && (int)h_offsets.size() >= num_negs) {
+        // the rows where diag_row adds each offset's term (TaiChi.cu:1014-1023)
+        const int xs = h_xStart[0], xe = h_xStop[0];
+        d.dn = num_negs;
+        for (int i = 0; i < num_negs; ++i) {
+            const int off = h_offsets[i];
+            d.d_lo[i] = std::max(xs + std::max(0, -off), row_start);
+            d.d_hi[i] = std::min(xe - std::max(0, off), row_stop);
+            d.d_col[i] = h_yStart[0] - xs + off;
+        }
+    } else if (dia_shapes > 0) {
+        d.dgen = 1;
     }
+    // the rows kernel: a stream plan (every row at most kStreamRowMax words)
+    // of short rows, or any stream plan on request
+    d.rows = 0;
+    if (d.per_tile == 4 && !(params.flags & TC_FLAG_NO_ROWS))
+        d.rows = (params.flags & TC_FLAG_ROWS) || (M > 0 && nnz_csr <= (int64_t)tc::kRowsMeanMax * M && tc::kRowsByDefault);
+    d.rows_pair = d.rows && (params.flags & TC_FLAG_ROWS_PAIR) ? 1 : 0;
+    // CTAs resident at once (the stream kernel's many-tile build, the rows
+    // kernel): the CTA that starts when this one ends is about this far on
+    d.ahead = (params.flags & TC_FLAG_NO_PREFETCH) ? (1 << 30)
+            : (d.rows_pair ? tc::kRowsMinBlocks / 2 : d.rows ? tc::kRowsMinBlocks : tc::kStreamManyMinBlocks) *
+                  tc::num_sms();
     d.wtiles = d_wtiles;
     d.nwtiles = nwtiles;
     d.wlo = wlo;

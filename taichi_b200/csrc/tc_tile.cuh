@@ -106,6 +106,28 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// L2 prefetch of a[i0, i1) of a plan array (row pointers or CSR words),
+// rounded out to 16 bytes: the plan's arrays start 256-byte aligned and are
+// padded by 16 bytes past their last element, so the rounded span stays
+// inside the allocation.
+__device__ __forceinline__ void prefetch_span(const int *a, int i0, int i1)
+{
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(a + i0) & ~uintptr_t(15);
+    const uintptr_t hi = (reinterpret_cast<uintptr_t>(a + i1) + 15) & ~uintptr_t(15);
+    if (hi > lo) prefetch_l2(reinterpret_cast<const void *>(lo), (unsigned)(hi - lo));
+}
+
+// Row pointers and CSR words of rows [r0, r1), whose words are [z0, z1),
+// brought into L2 about a wave before the CTA that reads them starts: the
+// CTA's row-pointer and word loads then hit L2 instead of waiting on HBM,
+// and the HBM reads run ahead of the dependent load chains.  Immutable plan
+// data, so it may be issued at any time.
+__device__ __forceinline__ void prefetch_rows_ahead(const DevPlan &p, int r0, int r1, int z0, int z1)
+{
+    prefetch_span(p.rowptr, r0, r1 + 1);
+    prefetch_span(p.cols, z0, z1);
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll
@@ -704,12 +726,13 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
 #pragma unroll
     for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    if (SIGNED && p.diag1) {
+    if (SIGNED && p.dn == 1) {
         // one dense diagonal: which rows have its term comes from the launch
         // parameters (no plan reads on the chain); the terms and order of
         // diag_run4
-        const float *xd = x + g + p.d1_col;
-        if (g >= p.d1_lo && g + 4 <= p.d1_hi && (p.d1_col & 3) == 0) {   // x is 16-byte aligned
+        const int lo = p.d_lo[0], hi = p.d_hi[0], col = p.d_col[0];
+        const float *xd = x + g + col;
+        if (g >= lo && g + 4 <= hi && (col & 3) == 0) {   // x is 16-byte aligned
             float d[4];
             asm("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];"
                 : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3]) : "l"(xd));
@@ -718,10 +741,10 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
         } else {
             float d[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) d[u] = g + u >= p.d1_lo && g + u < p.d1_hi ? ldx(xd + u) : 0.f;
+            for (int u = 0; u < 4; ++u) d[u] = g + u >= lo && g + u < hi ? ldx(xd + u) : 0.f;
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (g + u >= p.d1_lo && g + u < p.d1_hi) acc[u] += d[u];
+                if (g + u >= lo && g + u < hi) acc[u] += d[u];
         }
     } else if (SIGNED) {
         diag_run4(p, x, dc, g, 4, acc);

@@ -351,6 +351,68 @@ def test_spmv_mesh2048_full_size(tc, dev):
     check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/window")
     np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_stream)
     plan.close()
+    for flags, kernel in ((tc.TC_FLAG_ROWS, "rows"), (tc.TC_FLAG_ROWS | tc.TC_FLAG_ROWS_PAIR, "rows"),
+                          (tc.TC_FLAG_NO_ROWS, "stream")):
+        plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=flags))
+        assert tc.KERNEL_NAMES[plan.info()["kernel"]] == kernel
+        check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/%s/%#x" % (kernel, flags))
+        np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_stream)
+        plan.close()
+
+
+@pytest.mark.parametrize("pair", [0, 1], ids=["one", "pair"])
+@pytest.mark.parametrize("case", PARTITION_CASES, ids=[c["name"] for c in PARTITION_CASES])
+def test_rows_kernel(tc, dev, case, pair):
+    """The rows kernel (one row per thread, words straight from global
+    memory) on every matrix whose rows all fit a stream tile -- no shape,
+    one shape of one or several offsets, several shapes (the per-row shape
+    search), plain and hybrid words: against the oracle, and bit-identical to
+    the stream-tile kernel on the same format (same terms, same order)."""
+    M, N, rp, col = cases.matrix(case)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    if np.diff(fmt["csrRow"]).max(initial=0) > 128:
+        pytest.skip("rows longer than a stream tile takes")
+    base = tc.TC_FLAG_NO_DIRECT | tc.TC_FLAG_NO_WIDE | tc.TC_FLAG_ROWS_STRIDED | tc.TC_FLAG_NO_WINDOW
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(
+        flags=base | tc.TC_FLAG_ROWS | (tc.TC_FLAG_ROWS_PAIR if pair else 0)))
+    assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "rows", plan.info()
+    label = "%s/rows%d" % (case["name"], 1 + pair)
+    check_plan(plan, fmt, M, N, rp, col, dev, label)
+    x = np.random.default_rng(6).uniform(-1, 1, N).astype(np.float32)
+    y_rows = run_spmv(plan, x, M, dev)
+    plan.close()
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=base | tc.TC_FLAG_NO_ROWS))
+    assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "stream", plan.info()
+    np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_rows, err_msg=label)
+    plan.close()
+
+
+def test_rows_kernel_unaligned_and_chained(tc, dev):
+    """x and y at odd addresses, and chained multiplies v <- A v under
+    programmatic dependent launch (x of each multiply is the y of the one
+    before): the rows kernel reads x only after the wait."""
+    import torch
+    M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=9)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=tc.TC_FLAG_ROWS))
+    assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "rows"
+    x = np.random.default_rng(8).integers(-8, 9, N).astype(np.float32)
+    xb = torch.zeros(N + 1, dtype=torch.float32, device=dev)
+    xb[1:] = to_dev(x, dev)
+    yb = torch.full((M + 1,), float("nan"), dtype=torch.float32, device=dev)
+    plan.spmv(xb[1:].data_ptr(), yb[1:].data_ptr())
+    torch.cuda.synchronize()
+    want = oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64))
+    np.testing.assert_array_equal(yb[1:].cpu().numpy().astype(np.float64), want)
+    # chained: integers stay exact for 3 steps (|v| grows at most 9x a step)
+    v = [to_dev(np.sign(x), dev)] + [torch.empty(M, device=dev) for _ in range(3)]
+    for k in range(3):
+        plan.spmv(v[k], v[k + 1])
+    torch.cuda.synchronize()
+    w = np.sign(x).astype(np.float64)
+    for k in range(3):
+        w = oracle.spmv_csr_f64(M, rp, col, w)
+        np.testing.assert_array_equal(v[k + 1].cpu().numpy().astype(np.float64), w, err_msg="step %d" % k)
+    plan.close()
 
 
 WINDOW_CASES = [c for c in PARTITION_CASES if c["name"] in
