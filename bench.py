@@ -213,11 +213,13 @@ def run_ours(args, rank, world, local_rank):
     if args.wide_bounds:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_BOUNDS
     for on, f in ((args.rows, tc.TC_FLAG_ROWS), (args.no_rows, tc.TC_FLAG_NO_ROWS),
-                  (args.rows_pair, tc.TC_FLAG_ROWS_PAIR), (args.no_prefetch, tc.TC_FLAG_NO_PREFETCH)):
+                  (args.no_prefetch, tc.TC_FLAG_NO_PREFETCH)):
         if on:
             over["flags"] = over.get("flags", 0) | f
     if args.tile_nnz is not None:
         over["tile_nnz"] = args.tile_nnz
+    if args.rows_w is not None:
+        over["rows_w"] = args.rows_w
     if args.ctas_per_sm is not None:
         over["ctas_per_sm"] = args.ctas_per_sm
     prm = tc.params(**over)
@@ -715,7 +717,7 @@ def main():
                     help="wide plans: tile word ranges in the launch parameters, words staged in shared memory")
     ap.add_argument("--rows", action="store_true", help="stream plans: the rows kernel whatever the row lengths")
     ap.add_argument("--no-rows", action="store_true", help="stream plans: never the rows kernel")
-    ap.add_argument("--rows-pair", action="store_true", help="the rows kernel: two rows per thread")
+    ap.add_argument("--rows-w", type=int, default=None, help="the rows kernel: words of a row loaded together")
     ap.add_argument("--no-prefetch", action="store_true",
                     help="stream / rows kernels: no L2 prefetch of the operands a wave ahead")
     ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")

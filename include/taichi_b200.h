@@ -60,6 +60,8 @@ typedef struct tc_params {
                              (entry-parallel gather into shared memory, then
                              row sums), one CTA per tile (2)                   */
     int flags;            /* TC_FLAG_*                                         */
+    int rows_w;           /* rows kernel: words of a row loaded together, 4, 6
+                             or 8 (0: the least that holds 90 % of the rows)   */
 } tc_params;
 
 #define TC_FLAG_NO_PARTITION 0x1  /* skip the morphology: plain CSR plan      */
@@ -91,8 +93,6 @@ typedef struct tc_params {
                                      the rows' mean length                  */
 #define TC_FLAG_NO_ROWS      0x800 /* plans of stream tiles only: never run
                                      the rows kernel                        */
-#define TC_FLAG_ROWS_PAIR    0x1000 /* the rows kernel runs two rows per
-                                     thread (half the CTAs)                 */
 #define TC_FLAG_NO_PREFETCH  0x2000 /* stream and rows kernels: no L2
                                      prefetch of the operands of the CTA a
                                      wave ahead                             */

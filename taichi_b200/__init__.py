@@ -28,7 +28,6 @@ TC_FLAG_WIDE_BOUNDS = 0x100
 TC_FLAG_WIDE_FIXED = 0x200
 TC_FLAG_ROWS = 0x400
 TC_FLAG_NO_ROWS = 0x800
-TC_FLAG_ROWS_PAIR = 0x1000
 TC_FLAG_NO_PREFETCH = 0x2000
 
 _IP = C.POINTER(C.c_int)
@@ -44,7 +43,7 @@ class Params(C.Structure):
     _fields_ = [("thumb_height", C.c_int), ("open_len", C.c_int), ("eye_size", C.c_int),
                 ("min_contour", C.c_int), ("min_shape_side", C.c_int), ("density", C.c_double),
                 ("tile_rows", C.c_int), ("tile_nnz", C.c_int), ("max_lanes", C.c_int),
-                ("ctas_per_sm", C.c_int), ("tile_mode", C.c_int), ("flags", C.c_int)]
+                ("ctas_per_sm", C.c_int), ("tile_mode", C.c_int), ("flags", C.c_int), ("rows_w", C.c_int)]
 
 
 class Format(C.Structure):

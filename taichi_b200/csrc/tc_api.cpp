@@ -69,6 +69,7 @@ void tc_params_default(tc_params *p)
     p->ctas_per_sm = 4;
     p->tile_mode = 2;
     p->flags = 0;
+    p->rows_w = 0;
 }
 
 }  // extern "C"
@@ -88,6 +89,8 @@ tc_status tc::check_params(const tc_params &p)
         return fail(TC_ERR_INVALID, "ctas_per_sm %d outside [1, 32]", p.ctas_per_sm);
     if (p.max_lanes < 1 || p.max_lanes > 32 || (p.max_lanes & (p.max_lanes - 1)))
         return fail(TC_ERR_INVALID, "max_lanes %d is not a power of two in [1, 32]", p.max_lanes);
+    if (p.rows_w != 0 && p.rows_w != 4 && p.rows_w != 6 && p.rows_w != 8)
+        return fail(TC_ERR_INVALID, "rows_w %d is not 0, 4, 6 or 8", p.rows_w);
     return TC_OK;
 }
 

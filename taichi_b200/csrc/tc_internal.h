@@ -89,9 +89,8 @@ constexpr int kStream4Rows = 1024;    // most rows of a TILE_STREAM4 tile (a run
 constexpr int kDirectRows = 1024;     // most rows of a direct tile (TILE_DIRECT4)
 constexpr int kDirectWideBlock = 1024; // threads of the direct kernel's CTAs
 constexpr int kPlanDiags = 8;         // dense diagonals a plan can carry in its launch parameters
-constexpr int kRowsW = 8;             // CSR words of a row the rows kernel loads together
 constexpr int kRowsMeanMax = 12;      // rows kernel by default: mean CSR words per row at most this
-constexpr bool kRowsByDefault = false;
+constexpr bool kRowsByDefault = true;
 constexpr int kDirectWideRows = 4 * kDirectWideBlock;   // most rows of a TILE_DIRECT_WIDE tile
 // A wide plan of at most kWideBoundTiles whole tiles passes each tile's
 // first CSR word in the launch parameters (WideBounds), so a CTA loads its
@@ -140,7 +139,8 @@ struct DevPlan {
     int dn, dgen;
     int d_lo[kPlanDiags], d_hi[kPlanDiags], d_col[kPlanDiags];
     int rows;               // stream plan run by the rows kernel (one row per thread)
-    int rows_pair;          // the rows kernel's CTAs run two strips of rows
+    int rows_w;             // the rows kernel's words loaded together (4, 6 or 8: from the usual row length)
+    int pos;                // hybrid plan whose words are all additions (no holes)
     int ahead;              // stream / rows kernels: CTA b prefetches the operands of CTA b + ahead
     int skew;               // stream tiles use skewed shared-memory slots (vslot)
     // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
@@ -180,6 +180,8 @@ struct tc_plan {
     int *d_err = nullptr;
     int wide_rows = 0;                   // rows of each wide direct tile
     int stream_skew = 0;                 // the plan's usual row length is a multiple of 8
+    int rows_w = 8;                      // the rows kernel's words in flight (the usual row length, 4 / 6 / 8)
+    int all_pos = 0;                     // hybrid plan with no holes (every word an addition)
     // window plan (tc_window.cu); nwtiles == 0 when the plan has none
     tc::Tile *d_wtiles = nullptr;
     int nwtiles = 0, wlo = 0, whi = 0, w_rp = 0, w_cw = 0, w_xw = 0, w_stages = 0, w_grid = 0;

@@ -223,7 +223,9 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
 // window is one aligned 16 KB prefetch; the launch picks it from those facts.
 // (One kernel holding both paths behind a per-tile branch ran the full tiles
 // 0.8 µs slower per R-MAT scale 20 multiply than this split.)
-template <bool SIGNED, bool FULL>
+// POS (with SIGNED and FULL): every word of the plan is an addition (no
+// holes in its dense diagonals), so the gathers skip the sign.
+template <bool SIGNED, bool FULL, bool POS = false>
 __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan p, const float *__restrict__ x,
                                                                      float *__restrict__ y)
 {
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
             wait_prior_grid(x, y);
             return;
         }
-        direct_run_full<SIGNED>(p, dc, x, y, row0 + 4 * threadIdx.x);
+        direct_run_full<SIGNED, POS>(p, dc, x, y, row0 + 4 * threadIdx.x);
     } else {
         if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
         direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
@@ -251,8 +253,8 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
 
 // The multiply of a stream plan of short rows, one row per thread, read
 // straight from global memory: no tile records, shared memory or barriers.
-// A CTA runs RPT strips of kBlock consecutive rows (coalesced row pointers
-// and y stores).  Each thread loads its row's first kRowsW words together
+// A CTA runs kBlock consecutive rows (coalesced row pointers and y
+// stores).  Each thread loads its row's first W words together
 // (immutable plan data, before griddepcontrol.wait), then their gathers and
 // its dense-diagonal terms together, and adds the diagonal terms (offset
 // order), then the words (stored order), then any further words four at a
@@ -261,80 +263,70 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
 // of word w of its 32 rows touches the few cache lines holding those rows,
 // and its later words hit L1.  Against the stream tiles it spends no
 // instructions on parking terms in shared memory and no barrier waits.
-template <bool SIGNED, int RPT>
-__global__ void __launch_bounds__(kBlock, RPT == 1 ? kRowsMinBlocks : kRowsMinBlocks / 2)
+template <bool SIGNED, int W>
+__global__ void __launch_bounds__(kBlock, kRowsMinBlocks)
     spmv_rows_kernel(DevPlan p, const float *__restrict__ x, float *__restrict__ y)
 {
     allow_next_grid();
-    const int r0 = blockIdx.x * (kBlock * RPT) + threadIdx.x;
-    // thread 0 also brings into L2 the operands of the strip a wave later
-    const bool ahead = threadIdx.x == 0 && blockIdx.x + p.ahead < gridDim.x;
+    const int r = blockIdx.x * kBlock + threadIdx.x;
+    // warp 0 also brings into L2 the x window of the strip and the operands
+    // of the strip a wave later (thread 0; the other warps skip it whole)
+    const bool lead = threadIdx.x < 32;
+    const bool ahead = lead && blockIdx.x + p.ahead < gridDim.x;
     int za = 0, zb = 0;
-    if (threadIdx.x == 0) prefetch_x_window(x, p.N, r0, kBlock * RPT);
-    int b[RPT], e[RPT], c[RPT][kRowsW];
-#pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-        const int r = r0 + k * kBlock;
-        b[k] = r < p.M ? __ldg(p.rowptr + r) : 0;
-        e[k] = r < p.M ? __ldg(p.rowptr + r + 1) : 0;
-    }
+    if (lead && threadIdx.x == 0) prefetch_x_window(x, p.N, r, kBlock);
+    const int b = r < p.M ? __ldg(p.rowptr + r) : 0;
+    const int e = r < p.M ? __ldg(p.rowptr + r + 1) : 0;
     if (ahead) {
-        const int ra = (blockIdx.x + p.ahead) * (kBlock * RPT);
+        const int ra = (blockIdx.x + p.ahead) * kBlock;
         za = __ldg(p.rowptr + ra);
-        zb = __ldg(p.rowptr + min(ra + kBlock * RPT, p.M));
+        zb = __ldg(p.rowptr + min(ra + kBlock, p.M));
     }
+    int c[W];
 #pragma unroll
-    for (int k = 0; k < RPT; ++k)
-#pragma unroll
-        for (int w = 0; w < kRowsW; ++w) c[k][w] = b[k] + w < e[k] ? __ldg(p.cols + b[k] + w) : 0;
-    if (ahead) {
-        const int ra = (blockIdx.x + p.ahead) * (kBlock * RPT);
-        prefetch_rows_ahead(p, ra, min(ra + kBlock * RPT, p.M), za, zb);
+    for (int w = 0; w < W; ++w) c[w] = b + w < e ? __ldg(p.cols + b + w) : 0;
+    if (ahead && threadIdx.x == 0) {
+        const int ra = (blockIdx.x + p.ahead) * kBlock;
+        prefetch_rows_ahead(p, ra, min(ra + kBlock, p.M), za, zb);
     }
     wait_prior_grid(x, y);
-    float v[RPT][kRowsW];
+    float v[W];
 #pragma unroll
-    for (int k = 0; k < RPT; ++k)
-#pragma unroll
-        for (int w = 0; w < kRowsW; ++w) v[k][w] = b[k] + w < e[k] ? gather<SIGNED>(x, c[k][w]) : 0.f;
-#pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-        const int r = r0 + k * kBlock;
-        float acc = 0.f;
-        if (SIGNED && p.dgen) {
-            acc = diag_row(p, x, r);
-        } else if (SIGNED) {
+    for (int w = 0; w < W; ++w) v[w] = b + w < e ? gather<SIGNED>(x, c[w]) : 0.f;
+    float acc = 0.f;
+    if (SIGNED && p.dgen) {
+        acc = diag_row(p, x, r);
+    } else if (SIGNED) {
 #pragma unroll 1
-            for (int i = 0; i < p.dn; i += 4) {
-                float d[4];
-                bool in[4];
+        for (int i = 0; i < p.dn; i += 4) {                      // the plan's offsets in order
+            float d[4];
+            bool in[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    in[u] = i + u < p.dn && r >= p.d_lo[i + u] && r < p.d_hi[i + u];
-                    d[u] = in[u] ? ldx(x + r + p.d_col[i + u]) : 0.f;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    if (in[u]) acc += d[u];
+            for (int u = 0; u < 4; ++u) {
+                in[u] = i + u < p.dn && r >= p.d_lo[i + u] && r < p.d_hi[i + u];
+                d[u] = in[u] ? ldx(x + r + p.d_col[i + u]) : 0.f;
             }
-        }
-#pragma unroll
-        for (int w = 0; w < kRowsW; ++w)
-            if (b[k] + w < e[k]) acc += v[k][w];
-#pragma unroll 1
-        for (int j = b[k] + kRowsW; j < e[k]; j += 4) {            // longer rows
-            int cc[4];
-            float vv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) cc[u] = j + u < e[k] ? __ldg(p.cols + j + u) : 0;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) vv[u] = j + u < e[k] ? gather<SIGNED>(x, cc[u]) : 0.f;
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (j + u < e[k]) acc += vv[u];
+                if (in[u]) acc += d[u];
         }
-        if (r < p.M) y[r] = acc;
     }
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+        if (b + w < e) acc += v[w];
+#pragma unroll 1
+    for (int j = b + W; j < e; j += 4) {                            // longer rows
+        int cc[4];
+        float vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) cc[u] = j + u < e ? __ldg(p.cols + j + u) : 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) vv[u] = j + u < e ? gather<SIGNED>(x, cc[u]) : 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (j + u < e) acc += vv[u];
+    }
+    if (r < p.M) y[r] = acc;
 }
 
 // The multiply of a stream plan: one CTA per tile, no shared-memory stages
@@ -544,13 +536,15 @@ static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const flo
                       ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
     if (dp.per_tile == 3 && full && wb && dp.wide_rows == kDirectWideRows && dp.M % kDirectWideRows == 0)
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_bounds_kernel<SIGNED>, dp, *wb, x, y));
+    else if (dp.per_tile == 3 && full && SIGNED && dp.pos)
+        TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true, true>, dp, x, y));
     else if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
     else if (dp.per_tile == 3) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, false>, dp, x, y));
     else if (dp.per_tile == 4 && dp.rows) {
-        const bool pair = (dp.rows_pair != 0);
-        cfg.gridDim = dim3((unsigned)((dp.M + kBlock * (pair ? 2 : 1) - 1) / (kBlock * (pair ? 2 : 1))));
-        if (pair) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 2>, dp, x, y));
-        else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 1>, dp, x, y));
+        cfg.gridDim = dim3((unsigned)((dp.M + kBlock - 1) / kBlock));
+        if (dp.rows_w <= 4) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 4>, dp, x, y));
+        else if (dp.rows_w <= 6) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 6>, dp, x, y));
+        else TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_rows_kernel<SIGNED, 8>, dp, x, y));
     }
     else if (dp.per_tile == 4 && dp.ntiles > kLeanMinBlocks * num_sms())
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_stream_kernel<SIGNED, true>, dp, x, y));
@@ -645,12 +639,12 @@ tc::DevPlan tc_plan::dev_plan() const
     d.rows = 0;
     if (d.per_tile == 4 && !(params.flags & TC_FLAG_NO_ROWS))
         d.rows = (params.flags & TC_FLAG_ROWS) || (M > 0 && nnz_csr <= (int64_t)tc::kRowsMeanMax * M && tc::kRowsByDefault);
-    d.rows_pair = d.rows && (params.flags & TC_FLAG_ROWS_PAIR) ? 1 : 0;
+    d.rows_w = params.rows_w ? params.rows_w : rows_w;
+    d.pos = hybrid && all_pos ? 1 : 0;
     // CTAs resident at once (the stream kernel's many-tile build, the rows
     // kernel): the CTA that starts when this one ends is about this far on
     d.ahead = (params.flags & TC_FLAG_NO_PREFETCH) ? (1 << 30)
-            : (d.rows_pair ? tc::kRowsMinBlocks / 2 : d.rows ? tc::kRowsMinBlocks : tc::kStreamManyMinBlocks) *
-                  tc::num_sms();
+            : (d.rows ? tc::kRowsMinBlocks : tc::kStreamManyMinBlocks) * tc::num_sms();
     d.wtiles = d_wtiles;
     d.nwtiles = nwtiles;
     d.wlo = wlo;
@@ -731,6 +725,25 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
         }
         const int mode = (int)(std::max_element(h.begin() + 1, h.end()) - h.begin());
         p->stream_skew = h[mode] > 0 && mode % 8 == 0;
+        // a hybrid plan with no holes: every word adds its term
+        p->all_pos = 1;
+        if (p->hybrid)
+            for (int64_t j = 0; j < csrRow[M] && p->all_pos; ++j) p->all_pos = csrCol[j] & 1;
+        // the rows kernel loads W words of a row together: the least of 4, 6, 8
+        // that holds 90 % of the rows whole
+        int64_t tot = 0, upto = 0;
+        for (int L = 0; L <= kStreamRowMax; ++L) tot += h[L];
+        p->rows_w = 8;
+        for (int L = 0, w = 4; L <= 8 && tot > 0; ++L) {
+            upto += h[L];
+            if (L == w) {
+                if (upto * 10 >= tot * 9) {
+                    p->rows_w = w;
+                    break;
+                }
+                w += 2;
+            }
+        }
     }
     p->h_wide_nz.clear();
     if (p->ntiles_wide == p->ntiles && p->ntiles > 0 && p->ntiles <= kWideBoundTiles &&

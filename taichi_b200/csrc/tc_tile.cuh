@@ -54,6 +54,15 @@ __device__ __forceinline__ float gather(const float *__restrict__ x, int c)
     return ldx(x + c);
 }
 
+// gather() of a signed word known to be an addition (c & 1 set: a plan
+// with no holes in its dense diagonals), without the sign select.
+template <bool SIGNED, bool POS>
+__device__ __forceinline__ float gather_pos(const float *__restrict__ x, int c)
+{
+    if (SIGNED && POS) return ldx(x + (c >> 1));
+    return gather<SIGNED>(x, c);
+}
+
 // Programmatic dependent launch: a kernel reads only immutable plan data
 // before wait_prior_grid(); x is read and y written after it, when every grid
 // earlier in the stream has finished and its writes are visible.
@@ -711,7 +720,7 @@ __device__ __forceinline__ void direct_run(const DevPlan &p, int row0, int nr, i
 // The run of rows [g, g + 4) (g a multiple of 4, all four rows inside the
 // matrix, y 16-byte aligned): direct_run's terms and order without its edge
 // handling, for the full tiles of the direct kernel.
-template <bool SIGNED>
+template <bool SIGNED, bool POS = false>
 __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const float *__restrict__ x,
                                                 float *__restrict__ y, int g)
 {
@@ -724,7 +733,7 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
     wait_prior_grid(x, y);
     float v[kDirectW];
 #pragma unroll
-    for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather<SIGNED>(x, c[w]) : 0.f;
+    for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather_pos<SIGNED, POS>(x, c[w]) : 0.f;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     if (SIGNED && p.dn == 1) {
         // one dense diagonal: which rows have its term comes from the launch
@@ -755,7 +764,7 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
         for (int u = 0; u < 4; ++u)
             if (b[0] + w >= b[u] && b[0] + w < b[u + 1]) acc[u] += v[w];
     for (int j = b[0] + kDirectW; j < e4; ++j) {
-        const float z = gather<SIGNED>(x, __ldg(p.cols + j));
+        const float z = gather_pos<SIGNED, POS>(x, __ldg(p.cols + j));
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (j >= b[u] && j < b[u + 1]) acc[u] += z;

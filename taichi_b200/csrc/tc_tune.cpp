@@ -146,11 +146,13 @@ extern "C" tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const
         f.xStop = best_plan->h_xStop.data(); f.nDiasPtr = best_plan->h_nDiasPtr.data();
         f.neg_offsets = best_plan->h_offsets.data();
         f.csrRow = rp.data(); f.csrCol = cw.data();
-        // {tile_mode, tile_rows, max_lanes, ctas_per_sm, window flag}, most
-        // promising first (window flag: 0 the planner's choice, else forced
-        // on / off)
-        const int W = TC_FLAG_WINDOW, NW = TC_FLAG_NO_WINDOW;
-        const int cand[][5] = {{2, 1024, 32, 4, 0}, {2, 1024, 32, 4, W}, {2, 1024, 32, 4, NW},
+        // {tile_mode, tile_rows, max_lanes, ctas_per_sm, kernel flags}, most
+        // promising first (kernel flags: 0 the planner's choice, else the
+        // window or rows kernel forced on / off)
+        const int W = TC_FLAG_WINDOW, NW = TC_FLAG_NO_WINDOW, R = TC_FLAG_ROWS, NR = TC_FLAG_NO_ROWS;
+        const int KF = W | NW | R | NR;
+        const int cand[][5] = {{2, 1024, 32, 4, 0}, {2, 1024, 32, 4, R}, {2, 1024, 32, 4, NR},
+                               {2, 1024, 32, 4, W}, {2, 1024, 32, 4, NW},
                                {2, 512, 32, 4, W}, {2, 2048, 32, 4, 0}, {1, 1024, 32, 4, 0},
                                {0, 512, 32, 4, 0}, {2, 512, 32, 4, 0}, {0, 2048, 32, 4, 0},
                                {1, 1024, 8, 4, 0}, {0, 1024, 32, 8, 0}, {1, 1024, 32, 2, 0},
@@ -160,10 +162,10 @@ extern "C" tc_status tc_tune(int M, int N, int64_t nnz, const int *rowptr, const
                     tc_params q = best.params;
                     q.tile_mode = cnd[0]; q.tile_rows = cnd[1]; q.max_lanes = cnd[2];
                     q.ctas_per_sm = cnd[3];
-                    q.flags = (q.flags & ~(TC_FLAG_KEEP_HOST | W | NW)) | cnd[4];
+                    q.flags = (q.flags & ~(TC_FLAG_KEEP_HOST | KF)) | cnd[4];
                     if (q.tile_mode == best.params.tile_mode && q.tile_rows == best.params.tile_rows &&
                         q.max_lanes == best.params.max_lanes && q.ctas_per_sm == best.params.ctas_per_sm &&
-                        (q.flags & (W | NW)) == (best.params.flags & (W | NW)))
+                        (q.flags & KF) == (best.params.flags & KF))
                         continue;
                     tc_plan *p = nullptr;
                     st = tc_plan_from_format(M, N, &f, &q, stream, &p);

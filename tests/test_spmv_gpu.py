@@ -310,18 +310,21 @@ def test_chained_multiplies(tc, dev, name, mode):
 def test_stream_kernel_many_tiles(tc, dev):
     """Plans of stream tiles only, with more tiles than one wave at six CTAs
     per SM, run the 8-CTA stream kernel: the hybrid plan (signed words) and
-    the plain CSR plan of the same mesh, both against the oracle."""
+    the plain CSR plan of the same mesh, both against the oracle (the rows
+    kernel, the default for such short rows, turned off)."""
     import torch
     M, N, rp, col = matgen.mesh9(grid=512, permute_frac=0.02, seed=9)
-    no_window = tc.params(flags=tc.TC_FLAG_NO_WINDOW)
+    no_window = tc.params(flags=tc.TC_FLAG_NO_WINDOW | tc.TC_FLAG_NO_ROWS)
     plan = tc.Plan.from_csr(M, N, rp, col, prm=no_window)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     assert plan.info()["ntiles"] > 6 * sms and plan.info()["nwtiles"] == 0
+    assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "stream"
     check_plan(plan, plan.export(), M, N, rp, col, dev, "stream/many")
     x = np.random.default_rng(3).uniform(-1, 1, N).astype(np.float32)
     y_many = run_spmv(plan, x, M, dev)
     plan.close()
-    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=tc.TC_FLAG_NO_WINDOW), partition=False)
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=no_window, partition=False)
+    assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "stream"
     y_plain = run_spmv(plan, x, M, dev)
     plan.close()
     y64 = oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64))
@@ -341,8 +344,9 @@ def test_spmv_mesh2048_full_size(tc, dev):
     plan = tc.Plan.from_csr(M, N, rp, col)
     info = plan.info()
     assert info["dia_shapes"] == 1 and info["nwtiles"] == 0, info
+    assert tc.KERNEL_NAMES[info["kernel"]] == "rows", info        # short rows: the rows kernel
     fmt = plan.export()
-    check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/stream")
+    check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/default")
     x = np.random.default_rng(17).uniform(-1, 1, N).astype(np.float32)
     y_stream = run_spmv(plan, x, M, dev)
     plan.close()
@@ -351,7 +355,7 @@ def test_spmv_mesh2048_full_size(tc, dev):
     check_plan(plan, fmt, M, N, rp, col, dev, "mesh2048/window")
     np.testing.assert_array_equal(run_spmv(plan, x, M, dev), y_stream)
     plan.close()
-    for flags, kernel in ((tc.TC_FLAG_ROWS, "rows"), (tc.TC_FLAG_ROWS | tc.TC_FLAG_ROWS_PAIR, "rows"),
+    for flags, kernel in ((tc.TC_FLAG_ROWS, "rows"), (tc.TC_FLAG_ROWS | tc.TC_FLAG_NO_PREFETCH, "rows"),
                           (tc.TC_FLAG_NO_ROWS, "stream")):
         plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=flags))
         assert tc.KERNEL_NAMES[plan.info()["kernel"]] == kernel
@@ -360,9 +364,9 @@ def test_spmv_mesh2048_full_size(tc, dev):
         plan.close()
 
 
-@pytest.mark.parametrize("pair", [0, 1], ids=["one", "pair"])
+@pytest.mark.parametrize("w", [4, 6, 8])
 @pytest.mark.parametrize("case", PARTITION_CASES, ids=[c["name"] for c in PARTITION_CASES])
-def test_rows_kernel(tc, dev, case, pair):
+def test_rows_kernel(tc, dev, case, w):
     """The rows kernel (one row per thread, words straight from global
     memory) on every matrix whose rows all fit a stream tile -- no shape,
     one shape of one or several offsets, several shapes (the per-row shape
@@ -373,10 +377,9 @@ def test_rows_kernel(tc, dev, case, pair):
     if np.diff(fmt["csrRow"]).max(initial=0) > 128:
         pytest.skip("rows longer than a stream tile takes")
     base = tc.TC_FLAG_NO_DIRECT | tc.TC_FLAG_NO_WIDE | tc.TC_FLAG_ROWS_STRIDED | tc.TC_FLAG_NO_WINDOW
-    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(
-        flags=base | tc.TC_FLAG_ROWS | (tc.TC_FLAG_ROWS_PAIR if pair else 0)))
+    plan = tc.Plan.from_format(M, N, fmt, prm=tc.params(flags=base | tc.TC_FLAG_ROWS, rows_w=w))
     assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "rows", plan.info()
-    label = "%s/rows%d" % (case["name"], 1 + pair)
+    label = "%s/rows_w%d" % (case["name"], w)
     check_plan(plan, fmt, M, N, rp, col, dev, label)
     x = np.random.default_rng(6).uniform(-1, 1, N).astype(np.float32)
     y_rows = run_spmv(plan, x, M, dev)
