@@ -296,6 +296,19 @@ __global__ void __launch_bounds__(kBlock, kRowsMinBlocks)
     float acc = 0.f;
     if (SIGNED && p.dgen) {
         acc = diag_row(p, x, r);
+    } else if (SIGNED && p.dn <= 4) {
+        // the plan's offsets in order, named by constant indices (operands
+        // straight from the parameter bank)
+        float d[4];
+        bool in[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            in[u] = u < p.dn && r >= p.d_lo[u] && r < p.d_hi[u];
+            d[u] = in[u] ? ldx(x + r + p.d_col[u]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (in[u]) acc += d[u];
     } else if (SIGNED) {
 #pragma unroll 1
         for (int i = 0; i < p.dn; i += 4) {                      // the plan's offsets in order

@@ -515,6 +515,19 @@ __device__ __forceinline__ float diag_tile_row(const DevPlan &p, const float *__
 {
     if (dc == kDiagNone) return 0.f;
     if (dc == kDiagGeneral) return diag_row(p, x, r);
+    if (p.dn > 0 && p.dn <= 4) {
+        // the plan's one shape, every offset inside it for this tile's rows:
+        // the columns' shifts come with the plan descriptor (no shape or
+        // offset reads), offsets in order
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = u < p.dn ? ldx(x + r + p.d_col[u]) : 0.f;
+        float acc = 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (u < p.dn) acc += v[u];
+        return acc;
+    }
     const int4 sh = __ldg(p.shapes + dc - 1);
     const int2 dr = __ldg(p.shape_dias + dc - 1);
     const float *__restrict__ xr = x + (r - sh.x + sh.z);
