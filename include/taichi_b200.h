@@ -95,7 +95,8 @@ typedef struct tc_params {
                                      the rows kernel                        */
 #define TC_FLAG_NO_PREFETCH  0x2000 /* stream and rows kernels: no L2
                                      prefetch of the operands of the CTA a
-                                     wave ahead                             */
+                                     wave ahead; wide kernel: no L2 prefetch
+                                     of a tile's CSR words                  */
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */

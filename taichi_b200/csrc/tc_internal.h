@@ -142,6 +142,7 @@ struct DevPlan {
     int rows_w;             // the rows kernel's words loaded together (4, 6 or 8: from the usual row length)
     int pos;                // hybrid plan whose words are all additions (no holes)
     int ahead;              // stream / rows kernels: CTA b prefetches the operands of CTA b + ahead
+    int prefetch;           // wide kernel: each CTA prefetches its tile's CSR words into L2
     int skew;               // stream tiles use skewed shared-memory slots (vslot)
     // window plan (nwtiles > 0): the multiply runs the window kernel over wtiles
     const Tile *wtiles;

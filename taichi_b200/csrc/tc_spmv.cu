@@ -239,7 +239,15 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     // rows have the term
     const int dc = SIGNED && p.dn != 1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
     if (FULL) {
-        if (threadIdx.x == 0) prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
+        if (threadIdx.x == 0) {
+            prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
+            if (p.prefetch) {
+                // the tile's CSR words, so that the runs' word loads, which
+                // wait for their row pointers, find them in L2
+                const Tile t = p.tiles[blockIdx.x];
+                prefetch_span(p.cols, t.nz0, t.nz0 + t.nnz);
+            }
+        }
         if (4 * (int)threadIdx.x >= nr) {
             wait_prior_grid(x, y);
             return;
@@ -656,6 +664,7 @@ tc::DevPlan tc_plan::dev_plan() const
     d.pos = hybrid && all_pos ? 1 : 0;
     // CTAs resident at once (the stream kernel's many-tile build, the rows
     // kernel): the CTA that starts when this one ends is about this far on
+    d.prefetch = (params.flags & TC_FLAG_NO_PREFETCH) ? 0 : 1;
     d.ahead = (params.flags & TC_FLAG_NO_PREFETCH) ? (1 << 30)
             : (d.rows ? tc::kRowsMinBlocks : tc::kStreamManyMinBlocks) * tc::num_sms();
     d.wtiles = d_wtiles;
