@@ -213,7 +213,7 @@ def run_ours(args, rank, world, local_rank):
     if args.wide_bounds:
         over["flags"] = over.get("flags", 0) | tc.TC_FLAG_WIDE_BOUNDS
     for on, f in ((args.rows, tc.TC_FLAG_ROWS), (args.no_rows, tc.TC_FLAG_NO_ROWS),
-                  (args.no_prefetch, tc.TC_FLAG_NO_PREFETCH)):
+                  (args.no_prefetch, tc.TC_FLAG_NO_PREFETCH), (args.no_param_starts, tc.TC_FLAG_NO_PARAM_STARTS)):
         if on:
             over["flags"] = over.get("flags", 0) | f
     if args.tile_nnz is not None:
@@ -718,6 +718,8 @@ def main():
     ap.add_argument("--rows", action="store_true", help="stream plans: the rows kernel whatever the row lengths")
     ap.add_argument("--no-rows", action="store_true", help="stream plans: never the rows kernel")
     ap.add_argument("--rows-w", type=int, default=None, help="the rows kernel: words of a row loaded together")
+    ap.add_argument("--no-param-starts", action="store_true",
+                    help="wide plans: tile word ranges for the prefetch from the tile records")
     ap.add_argument("--no-prefetch", action="store_true",
                     help="stream / rows kernels: no L2 prefetch of the operands a wave ahead")
     ap.add_argument("--serve-contexts", type=int, default=4, help="served form: launch contexts (streams)")

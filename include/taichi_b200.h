@@ -97,6 +97,9 @@ typedef struct tc_params {
                                      prefetch of the operands of the CTA a
                                      wave ahead; wide kernel: no L2 prefetch
                                      of a tile's CSR words                  */
+#define TC_FLAG_NO_PARAM_STARTS 0x4000 /* wide plans: each tile's word
+                                     range from its tile record, not from
+                                     the launch parameters                  */
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */

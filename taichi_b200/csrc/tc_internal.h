@@ -101,6 +101,13 @@ constexpr int kWideWordQ = 2048;
 struct WideBounds {
     int nz[kWideBoundTiles + 1];
 };
+// A wide plan of at most kWideParamTiles tiles passes each tile's first CSR
+// word in the launch parameters (2 KB), so a CTA prefetches its tile's words
+// into L2 as it starts.
+constexpr int kWideParamTiles = 511;
+struct WideStarts {
+    int nz[kWideParamTiles + 1];
+};
 
 // Window plans (tc_window.cu): tiles of consecutive rows whose row pointers,
 // CSR words and x window are staged in shared memory by bulk copies.
@@ -190,6 +197,7 @@ struct tc_plan {
     std::vector<int> h_xStart, h_yStart, h_xStop, h_nDiasPtr, h_offsets;
     std::vector<int> h_rowptr, h_cols;   // only with TC_FLAG_KEEP_HOST
     std::vector<int> h_wide_nz;          // wide plans: first CSR word of each tile, and the end
+    std::vector<int> h_wide_z;           // the same for the word prefetch (WideStarts)
     // partition diagnostics
     double partition_ms = 0.0;
     int thumb_W = 0, thumb_H = 0;
@@ -240,7 +248,7 @@ constexpr int kItemMinBlocks = 5;
 // wb: the tiles' word bounds of a wide plan (nullptr: the kernels that read
 // them from the tile list).  launch_plan passes the plan's own.
 tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s,
-                      const WideBounds *wb = nullptr);
+                      const WideBounds *wb = nullptr, const WideStarts *ws = nullptr);
 tc_status launch_plan(const tc_plan *p, const float *x, float *y, cudaStream_t s);
 // Window plans (tc_window.cu): the planner (false when the matrix does not
 // qualify), the kernels' shared-memory setup and the launch.

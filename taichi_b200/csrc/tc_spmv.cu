@@ -224,7 +224,35 @@ __global__ void __launch_bounds__(kBlock) spmv_tiles_kernel(DevPlan p, const flo
 // (One kernel holding both paths behind a per-tile branch ran the full tiles
 // 0.8 µs slower per R-MAT scale 20 multiply than this split.)
 // POS (with SIGNED and FULL): every word of the plan is an addition (no
-// holes in its dense diagonals), so the gathers skip the sign.
+// holes in its dense diagonals), so the gathers skip the sign.  The FULL
+// body: z0 / z1, when z0 >= 0, are the tile's CSR word range as the launch
+// parameters give it (the prefetch of the words then goes out at once),
+// otherwise thread 0 reads the range from the tile record first.
+template <bool SIGNED, bool POS>
+__device__ __forceinline__ void wide_full(const DevPlan &p, const float *__restrict__ x, float *__restrict__ y,
+                                          int z0, int z1)
+{
+    const int row0 = blockIdx.x * p.wide_rows;
+    const int nr = min(p.wide_rows, p.M - row0);
+    const int dc = SIGNED && p.dn != 1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+    if (threadIdx.x == 0) {
+        prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
+        if (z0 >= 0) {
+            prefetch_span(p.cols, z0, z1);
+        } else if (p.prefetch) {
+            // the tile's CSR words, so that the runs' word loads, which wait
+            // for their row pointers, find them in L2
+            const Tile t = p.tiles[blockIdx.x];
+            prefetch_span(p.cols, t.nz0, t.nz0 + t.nnz);
+        }
+    }
+    if (4 * (int)threadIdx.x >= nr) {
+        wait_prior_grid(x, y);
+        return;
+    }
+    direct_run_full<SIGNED, POS>(p, dc, x, y, row0 + 4 * threadIdx.x);
+}
+
 template <bool SIGNED, bool FULL, bool POS = false>
 __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan p, const float *__restrict__ x,
                                                                      float *__restrict__ y)
@@ -232,31 +260,30 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     allow_next_grid();
     // wide tiles are laid out in order, p.wide_rows rows each (the last one
     // may be shorter), so the rows are known without waiting for the tile
-    // record; only the diagonal class comes from it
-    const int row0 = blockIdx.x * p.wide_rows;
-    const int nr = min(p.wide_rows, p.M - row0);
-    // a one-diagonal plan needs no tile record: the parameters say which
-    // rows have the term
-    const int dc = SIGNED && p.dn != 1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+    // record; only the diagonal class comes from it (a one-diagonal plan
+    // needs no tile record: the parameters say which rows have the term)
     if (FULL) {
-        if (threadIdx.x == 0) {
-            prefetch_l2(x + row0, (unsigned)nr * sizeof(float));
-            if (p.prefetch) {
-                // the tile's CSR words, so that the runs' word loads, which
-                // wait for their row pointers, find them in L2
-                const Tile t = p.tiles[blockIdx.x];
-                prefetch_span(p.cols, t.nz0, t.nz0 + t.nnz);
-            }
-        }
-        if (4 * (int)threadIdx.x >= nr) {
-            wait_prior_grid(x, y);
-            return;
-        }
-        direct_run_full<SIGNED, POS>(p, dc, x, y, row0 + 4 * threadIdx.x);
+        wide_full<SIGNED, POS>(p, x, y, -1, -1);
     } else {
+        const int row0 = blockIdx.x * p.wide_rows;
+        const int nr = min(p.wide_rows, p.M - row0);
+        const int dc = SIGNED && p.dn != 1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
         if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
         direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
     }
+}
+
+// The whole-tile wide kernel with each tile's first CSR word in the launch
+// parameters (plans of at most kWideParamTiles tiles): the prefetch of a
+// tile's words into L2 goes out when the CTA starts, together with its
+// row-pointer loads, instead of after a read of the tile record.
+template <bool SIGNED, bool POS>
+__global__ void __launch_bounds__(kDirectWideBlock, 2)
+    spmv_wide_starts_kernel(DevPlan p, const __grid_constant__ WideStarts ws, const float *__restrict__ x,
+                            float *__restrict__ y)
+{
+    allow_next_grid();
+    wide_full<SIGNED, POS>(p, x, y, ws.nz[blockIdx.x], ws.nz[blockIdx.x + 1]);
 }
 
 // The multiply of a stream plan of short rows, one row per thread, read
@@ -538,7 +565,8 @@ size_t stream_smem_bytes(const DevPlan &dp)
 }
 
 template <bool SIGNED>
-static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const float *x, float *y, cudaStream_t s)
+static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const WideStarts *ws, const float *x,
+                              float *y, cudaStream_t s)
 {
     if (dp.ntiles <= 0) return TC_OK;
     const size_t smem = dp.per_tile ? 0 : stream_smem_bytes(dp);
@@ -557,6 +585,10 @@ static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const flo
                       ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
     if (dp.per_tile == 3 && full && wb && dp.wide_rows == kDirectWideRows && dp.M % kDirectWideRows == 0)
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_bounds_kernel<SIGNED>, dp, *wb, x, y));
+    else if (dp.per_tile == 3 && full && ws && SIGNED && dp.pos)
+        TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_starts_kernel<SIGNED, true>, dp, *ws, x, y));
+    else if (dp.per_tile == 3 && full && ws)
+        TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_starts_kernel<SIGNED, false>, dp, *ws, x, y));
     else if (dp.per_tile == 3 && full && SIGNED && dp.pos)
         TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true, true>, dp, x, y));
     else if (dp.per_tile == 3 && full) TC_CUDA(cudaLaunchKernelEx(&cfg, spmv_wide_kernel<SIGNED, true>, dp, x, y));
@@ -576,19 +608,27 @@ static tc_status launch_tiles(const DevPlan &dp, const WideBounds *wb, const flo
     return TC_OK;
 }
 
-tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s, const WideBounds *wb)
+tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t s, const WideBounds *wb,
+                      const WideStarts *ws)
 {
     if (dp.M == 0) return TC_OK;
     if (dp.nwtiles > 0) return launch_window(dp, x, y, s);
-    return dp.hybrid ? launch_tiles<true>(dp, wb, x, y, s) : launch_tiles<false>(dp, wb, x, y, s);
+    return dp.hybrid ? launch_tiles<true>(dp, wb, ws, x, y, s) : launch_tiles<false>(dp, wb, ws, x, y, s);
 }
 
 tc_status launch_plan(const tc_plan *p, const float *x, float *y, cudaStream_t s)
 {
-    if (p->h_wide_nz.empty()) return launch_spmv(p->dev_plan(), x, y, s, nullptr);
-    WideBounds wb;
-    memcpy(wb.nz, p->h_wide_nz.data(), sizeof(int) * p->h_wide_nz.size());
-    return launch_spmv(p->dev_plan(), x, y, s, &wb);
+    if (!p->h_wide_nz.empty()) {
+        WideBounds wb;
+        memcpy(wb.nz, p->h_wide_nz.data(), sizeof(int) * p->h_wide_nz.size());
+        return launch_spmv(p->dev_plan(), x, y, s, &wb, nullptr);
+    }
+    if (!p->h_wide_z.empty()) {
+        WideStarts ws;
+        memcpy(ws.nz, p->h_wide_z.data(), sizeof(int) * p->h_wide_z.size());
+        return launch_spmv(p->dev_plan(), x, y, s, nullptr, &ws);
+    }
+    return launch_spmv(p->dev_plan(), x, y, s, nullptr, nullptr);
 }
 
 tc_status launch_spmm(const DevPlan &dp, const float *X, int ldx, int k, float *Y, int ldy,
@@ -772,6 +812,14 @@ tc_status plan_upload(tc_plan *p, const int *csrRow, const int *csrCol, cudaStre
         M % kDirectWideRows == 0 && (p->params.flags & TC_FLAG_WIDE_BOUNDS)) {
         for (const Tile &t : tiles) p->h_wide_nz.push_back(t.nz0);
         p->h_wide_nz.push_back(csrRow[M]);
+    }
+    // wide plans of few tiles: each tile's first word travels in the launch
+    // parameters, for the word prefetch
+    p->h_wide_z.clear();
+    if (p->ntiles_wide == p->ntiles && p->ntiles > 0 && p->ntiles <= kWideParamTiles &&
+        !(p->params.flags & (TC_FLAG_NO_PREFETCH | TC_FLAG_NO_PARAM_STARTS))) {
+        for (const Tile &t : tiles) p->h_wide_z.push_back(t.nz0);
+        p->h_wide_z.push_back(csrRow[M]);
     }
     // shared-memory stage sizes (ints, multiples of 4) from the largest tile
     int max_rows = 1, max_nnz = 0;

@@ -517,6 +517,29 @@ def test_wide_bounds_kernel(tc, dev):
         plan.close()
 
 
+@pytest.mark.parametrize("name", ["rmat16_selfloops", "rmat20", "rmat20_selfloops"])
+def test_wide_word_prefetch_forms(tc, dev, name):
+    """Wide plans prefetch each tile's CSR words into L2, the range taken
+    from the launch parameters (the default for at most 511 tiles), from the
+    tile record (TC_FLAG_NO_PARAM_STARTS), or not at all
+    (TC_FLAG_NO_PREFETCH): the same y bit for bit, exact for integer x
+    against the oracle; hybrid plans of one diagonal included."""
+    case = next(c for c in cases.MATRIX_CASES if c["name"] == name)
+    M, N, rp, col = cases.matrix(case)
+    x = np.random.default_rng(12).uniform(-1, 1, N).astype(np.float32)
+    ys = []
+    for flags in (0, tc.TC_FLAG_NO_PARAM_STARTS, tc.TC_FLAG_NO_PREFETCH):
+        plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(flags=flags))
+        assert tc.KERNEL_NAMES[plan.info()["kernel"]] == "wide", plan.info()
+        xi = np.random.default_rng(2).integers(-8, 9, N).astype(np.float64)
+        np.testing.assert_array_equal(run_spmv(plan, xi, M, dev).astype(np.float64),
+                                      oracle.spmv_csr_f64(M, rp, col, xi), err_msg="%s %#x" % (name, flags))
+        ys.append(run_spmv(plan, x, M, dev))
+        plan.close()
+    for y in ys[1:]:
+        np.testing.assert_array_equal(y, ys[0])
+
+
 @pytest.mark.parametrize("M", [1 << 18, 300004, 10001])
 def test_wide_balanced_tiles(tc, dev, M):
     """Wide tiles sized for two per SM (the default): a whole number of
