@@ -681,6 +681,15 @@ __device__ __forceinline__ void diag_run4(const DevPlan &p, const float *__restr
 // order either way.  (Two runs per thread with all loads in flight measured
 // slower on R-MAT; four run out of registers.)
 constexpr int kDirectW = 4;
+// The whole-run path (direct_run_full) keeps more words of a run in flight:
+// a run's words past the first W are walked one at a time, each a word load
+// then a gather, and on R-MAT scale 20 a run of 4 rows holds more than 4
+// words in 10 % of the runs -- 97 % of the warps -- more than 6 in 1.2 %
+// (32 % of the warps), more than 8 in 0.08 %.  Measured per multiply
+// (K = 2,000, one box): plain words W = 4 / 6 / 8: 4.74 / 4.52 / 4.71 µs;
+// signed words (self-loop plan) 5.29 / 5.30 / 5.20 µs.
+template <bool SIGNED>
+constexpr int direct_w_full() { return SIGNED ? 8 : 6; }
 
 // The run of rows [row0 + g, row0 + g + 4) of a direct tile of nr rows from
 // row0 and diagonal class dc, g a multiple of 4.
@@ -737,16 +746,17 @@ template <bool SIGNED, bool POS = false>
 __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const float *__restrict__ x,
                                                 float *__restrict__ y, int g)
 {
+    constexpr int kDirectWFull = direct_w_full<SIGNED>();
     const int4 r4 = __ldg(reinterpret_cast<const int4 *>(p.rowptr + g));
     const int e4 = __ldg(p.rowptr + g + 4);
     const int b[5] = {r4.x, r4.y, r4.z, r4.w, e4};
-    int c[kDirectW];
+    int c[kDirectWFull];
 #pragma unroll
-    for (int w = 0; w < kDirectW; ++w) c[w] = b[0] + w < e4 ? __ldg(p.cols + b[0] + w) : 0;
+    for (int w = 0; w < kDirectWFull; ++w) c[w] = b[0] + w < e4 ? __ldg(p.cols + b[0] + w) : 0;
     wait_prior_grid(x, y);
-    float v[kDirectW];
+    float v[kDirectWFull];
 #pragma unroll
-    for (int w = 0; w < kDirectW; ++w) v[w] = b[0] + w < e4 ? gather_pos<SIGNED, POS>(x, c[w]) : 0.f;
+    for (int w = 0; w < kDirectWFull; ++w) v[w] = b[0] + w < e4 ? gather_pos<SIGNED, POS>(x, c[w]) : 0.f;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     if (SIGNED && p.dn == 1) {
         // one dense diagonal: which rows have its term comes from the launch
@@ -772,11 +782,11 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
         diag_run4(p, x, dc, g, 4, acc);
     }
 #pragma unroll
-    for (int w = 0; w < kDirectW; ++w)
+    for (int w = 0; w < kDirectWFull; ++w)
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (b[0] + w >= b[u] && b[0] + w < b[u + 1]) acc[u] += v[w];
-    for (int j = b[0] + kDirectW; j < e4; ++j) {
+    for (int j = b[0] + kDirectWFull; j < e4; ++j) {
         const float z = gather_pos<SIGNED, POS>(x, __ldg(p.cols + j));
 #pragma unroll
         for (int u = 0; u < 4; ++u)
