@@ -325,21 +325,24 @@ __global__ void __launch_bounds__(kBlock, kRowsMinBlocks)
         prefetch_rows_ahead(p, ra, min(ra + kBlock, p.M), za, zb);
     }
     wait_prior_grid(x, y);
+    // every slot is loaded (a slot past the row holds word 0, a load of x[0]
+    // that is never added): no branch around the gathers
     float v[W];
 #pragma unroll
-    for (int w = 0; w < W; ++w) v[w] = b + w < e ? gather<SIGNED>(x, c[w]) : 0.f;
+    for (int w = 0; w < W; ++w) v[w] = gather<SIGNED>(x, c[w]);
     float acc = 0.f;
     if (SIGNED && p.dgen) {
         acc = diag_row(p, x, r);
     } else if (SIGNED && p.dn <= 4) {
         // the plan's offsets in order, named by constant indices (operands
-        // straight from the parameter bank)
+        // straight from the parameter bank); a row outside an offset's range
+        // loads x[0] for it and does not add it
         float d[4];
         bool in[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             in[u] = u < p.dn && r >= p.d_lo[u] && r < p.d_hi[u];
-            d[u] = in[u] ? ldx(x + r + p.d_col[u]) : 0.f;
+            d[u] = ldx(x + (in[u] ? r + p.d_col[u] : 0));
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(kBlock, kRowsMinBlocks)
 #pragma unroll
         for (int u = 0; u < 4; ++u) cc[u] = j + u < e ? __ldg(p.cols + j + u) : 0;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) vv[u] = j + u < e ? gather<SIGNED>(x, cc[u]) : 0.f;
+        for (int u = 0; u < 4; ++u) vv[u] = gather<SIGNED>(x, cc[u]);
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             if (j + u < e) acc += vv[u];
@@ -612,6 +615,12 @@ tc_status launch_spmv(const DevPlan &dp, const float *x, float *y, cudaStream_t 
                       const WideStarts *ws)
 {
     if (dp.M == 0) return TC_OK;
+    // no columns: no terms, and the kernels' unconditional loads of x[0]
+    // (slots past a row's words) would have no x to read
+    if (dp.N == 0) {
+        TC_CUDA(cudaMemsetAsync(y, 0, sizeof(float) * (size_t)dp.M, s));
+        return TC_OK;
+    }
     if (dp.nwtiles > 0) return launch_window(dp, x, y, s);
     return dp.hybrid ? launch_tiles<true>(dp, wb, ws, x, y, s) : launch_tiles<false>(dp, wb, ws, x, y, s);
 }

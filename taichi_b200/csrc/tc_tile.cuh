@@ -756,7 +756,7 @@ __device__ __forceinline__ void direct_run_full(const DevPlan &p, int dc, const 
     wait_prior_grid(x, y);
     float v[kDirectWFull];
 #pragma unroll
-    for (int w = 0; w < kDirectWFull; ++w) v[w] = b[0] + w < e4 ? gather_pos<SIGNED, POS>(x, c[w]) : 0.f;
+    for (int w = 0; w < kDirectWFull; ++w) v[w] = gather_pos<SIGNED, POS>(x, c[w]);   // past the run: x[0], not added
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     if (SIGNED && p.dn == 1) {
         // one dense diagonal: which rows have its term comes from the launch

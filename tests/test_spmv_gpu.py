@@ -216,6 +216,12 @@ def test_empty_and_tiny(tc, dev):
     # M == 0
     plan = tc.Plan.from_csr(0, 5, np.zeros(1, np.int32), np.zeros(0, np.int32), partition=False)
     plan.spmv(torch.ones(5, device=dev), torch.empty(0, device=dev))
+    # N == 0: no terms, y = 0, and x is never read
+    plan = tc.Plan.from_csr(10, 0, np.zeros(11, np.int32), np.zeros(0, np.int32), partition=False)
+    y = torch.full((10,), float("nan"), device=dev)
+    plan.spmv(torch.empty(0, device=dev), y)
+    torch.cuda.synchronize()
+    assert not y.cpu().numpy().any()
 
 
 def test_hybrid_without_csr_remainder(tc, dev):
