@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2)
 // stores).  Each thread loads its row's first W words together
 // (immutable plan data, before griddepcontrol.wait), then their gathers and
 // its dense-diagonal terms together, and adds the diagonal terms (offset
-// order), then the words (stored order), then any further words four at a
+// order), then the words (stored order), then any further words W at a
 // time: the terms and order of tile_rows_seq, so y is bit-identical to the
 // stream tiles'.  Consecutive lanes hold consecutive rows, so a warp's load
 // of word w of its 32 rows touches the few cache lines holding those rows,
@@ -366,15 +366,15 @@ __global__ void __launch_bounds__(kBlock, kRowsMinBlocks)
     for (int w = 0; w < W; ++w)
         if (b + w < e) acc += v[w];
 #pragma unroll 1
-    for (int j = b + W; j < e; j += 4) {                            // longer rows
-        int cc[4];
-        float vv[4];
+    for (int j = b + W; j < e; j += W) {                            // longer rows, W words at a time
+        int cc[W];
+        float vv[W];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) cc[u] = j + u < e ? __ldg(p.cols + j + u) : 0;
+        for (int u = 0; u < W; ++u) cc[u] = j + u < e ? __ldg(p.cols + j + u) : 0;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) vv[u] = gather<SIGNED>(x, cc[u]);
+        for (int u = 0; u < W; ++u) vv[u] = gather<SIGNED>(x, cc[u]);
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < W; ++u)
             if (j + u < e) acc += vv[u];
     }
     if (r < p.M) y[r] = acc;
