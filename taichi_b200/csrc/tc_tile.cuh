@@ -479,10 +479,15 @@ __device__ __forceinline__ void stream_gather(const float *__restrict__ x, float
                 sw.w[q] = i < sw.nq ? __ldg(sw.cq + i) : make_int4(0, 0, 0, 0);
             }
         }
+        // signed words: every slot is gathered -- a slot past the window
+        // holds word 0, a load of x[0] that is never stored -- so no branch
+        // surrounds the loads (mesh, stream tiles: 48.1 -> 45.7 us); plain
+        // words keep the branch (the unconditional form spills in the
+        // plain 8-CTA build)
         float4 v[kStreamQ];
 #pragma unroll
         for (int q = 0; q < kStreamQ; ++q) {
-            if (base + tid + q * kBlock < sw.nq) {
+            if (SIGNED || base + tid + q * kBlock < sw.nq) {
                 v[q].x = gather<SIGNED>(x, sw.w[q].x);
                 v[q].y = gather<SIGNED>(x, sw.w[q].y);
                 v[q].z = gather<SIGNED>(x, sw.w[q].z);
