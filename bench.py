@@ -365,9 +365,9 @@ def run_ours(args, rank, world, local_rank):
     warm_ms = ev0.elapsed_time(ev1) / 256
 
     # end to end through the public host API (pinned host buffers): every step
-    # copies its x in and its y out.  Headline: tc_spmv_host_async with two
-    # staging slots on two streams, so one step's x copy-in overlaps the
-    # previous step's y copy-out; also the synchronous tc_spmv_host.
+    # copies its x in and its y out.  Headline: tc_spmv_host_async with
+    # --e2e-slots staging slots on as many streams, so steps' x copy-ins
+    # overlap earlier steps' y copy-outs; also the synchronous tc_spmv_host.
     hxs = [torch.from_numpy(x_host).pin_memory() for _ in range(2)]
     hys = [torch.empty(M, dtype=torch.float32).pin_memory() for _ in range(2)]
     e2e_steps = max(3, min(args.steps, 400))
@@ -377,18 +377,22 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(e2e_steps):
         plan0.spmv_host(hxs[0], hys[0], stream=stream)
     sync_s = (time.perf_counter() - t0) / e2e_steps
-    streams = [stream, torch.cuda.Stream(dev)]
-    for i in range(4):
-        plan0.spmv_host_async(hxs[i & 1], hys[i & 1], i & 1, streams[i & 1])
+    S = args.e2e_slots
+    streams = [stream] + [torch.cuda.Stream(dev) for _ in range(S - 1)]
+    hxs = hxs + [torch.from_numpy(x_host).pin_memory() for _ in range(S - len(hxs))]
+    hys = hys + [torch.empty(M, dtype=torch.float32).pin_memory() for _ in range(S - len(hys))]
+    for i in range(2 * S):
+        plan0.spmv_host_async(hxs[i % S], hys[i % S], i % S, streams[i % S])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(e2e_steps):
-        plan0.spmv_host_async(hxs[i & 1], hys[i & 1], i & 1, streams[i & 1])
+        plan0.spmv_host_async(hxs[i % S], hys[i % S], i % S, streams[i % S])
     for s in streams:
         s.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     plan0.check()
-    assert np.array_equal(hys[0].numpy(), hys[1].numpy()), "pipelined host multiply mismatch"
+    for k in range(1, S):
+        assert np.array_equal(hys[0].numpy(), hys[k].numpy()), "pipelined host multiply mismatch"
     e2e_gbs = bytes_per / e2e_s / 1e9 * world
     e2e_sync_gbs = bytes_per / sync_s / 1e9 * world
 
@@ -436,7 +440,7 @@ def run_ours(args, rank, world, local_rank):
                          "peak_kind": peak_kind + " hbm_gbs (copy)", "traffic": traffic},
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 4 * N,
                     "d2h_bytes_per_step": 4 * M, "ms_per_step": e2e_s * 1e3,
-                    "api": "tc_spmv_host_async, 2 slots on 2 streams",
+                    "api": "tc_spmv_host_async, %d slots on %d streams" % (S, S),
                     "sync_value": round(e2e_sync_gbs, 3), "sync_api": "tc_spmv_host"},
             "gpu_launches": args.steps,
             "clocks": cl,
@@ -718,6 +722,8 @@ def main():
     ap.add_argument("--rows", action="store_true", help="stream plans: the rows kernel whatever the row lengths")
     ap.add_argument("--no-rows", action="store_true", help="stream plans: never the rows kernel")
     ap.add_argument("--rows-w", type=int, default=None, help="the rows kernel: words of a row loaded together")
+    ap.add_argument("--e2e-slots", type=int, default=4, choices=[1, 2, 3, 4],
+                    help="end-to-end figure: staging slots (and streams) of tc_spmv_host_async")
     ap.add_argument("--no-param-starts", action="store_true",
                     help="wide plans: tile word ranges for the prefetch from the tile records")
     ap.add_argument("--no-prefetch", action="store_true",

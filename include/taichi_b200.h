@@ -208,11 +208,15 @@ TC_API tc_status tc_spmv_f64(const tc_plan *plan, const double *d_x, double *d_y
  * waits.  Pinned host buffers give the full link bandwidth. */
 TC_API tc_status tc_spmv_host(const tc_plan *plan, const float *h_x, float *h_y, void *stream);
 
+#define TC_HOST_SLOTS 4  /* staging slots of tc_spmv_host_async */
+
 /* The same three steps enqueued on `stream` without waiting, through the
- * plan's staging slot `slot` (0 or 1; slot 0 is the one tc_spmv_host uses).
- * h_y holds y once the stream has reached this point.  Calls on one slot must
- * be ordered on the device (same stream, or an event between streams); two
- * slots on two streams let one call's x copy-in overlap another's y copy-out.
+ * plan's staging slot `slot` (0 .. TC_HOST_SLOTS-1; slot 0 is the one
+ * tc_spmv_host uses).  h_y holds y once the stream has reached this point.
+ * Calls on one slot must be ordered on the device (same stream, or an event
+ * between streams); slots on separate streams let one call's x copy-in
+ * overlap another's y copy-out, and with three or more a copy-in no longer
+ * waits for the copy-out two calls back.
  * No counterpart in the reference (its taichi_SpMV copies synchronously,
  * TaiChi.cu:1357-1420). */
 TC_API tc_status tc_spmv_host_async(const tc_plan *plan, const float *h_x, float *h_y, int slot,

@@ -507,7 +507,7 @@ class Plan:
         check(lib().tc_spmv_host(self._h, _ptr(x), _ptr(y), _stream(stream)))
 
     def spmv_host_async(self, x, y, slot, stream):
-        """Enqueue copy-in, multiply, copy-out through staging slot 0 or 1;
+        """Enqueue copy-in, multiply, copy-out through staging slot 0..3;
         y is ready once `stream` has reached this point."""
         check(lib().tc_spmv_host_async(self._h, _ptr(x), _ptr(y), slot, _stream(stream)))
 

@@ -175,10 +175,10 @@ tc_status tc_plan_destroy(tc_plan *p)
 {
     if (!p) return TC_OK;
     if (p->dev) cudaFree(p->dev);
-    if (p->d_xbuf) cudaFree(p->d_xbuf);
-    if (p->d_ybuf) cudaFree(p->d_ybuf);
-    if (p->d_xbuf1) cudaFree(p->d_xbuf1);
-    if (p->d_ybuf1) cudaFree(p->d_ybuf1);
+    for (int k = 0; k < TC_HOST_SLOTS; ++k) {
+        if (p->d_xbuf[k]) cudaFree(p->d_xbuf[k]);
+        if (p->d_ybuf[k]) cudaFree(p->d_ybuf[k]);
+    }
     delete p;
     return TC_OK;
 }
@@ -255,8 +255,8 @@ tc_status tc_spmv(const tc_plan *p, const float *d_x, float *d_y, void *stream)
 // slot `slot` (device x / y buffers allocated on first use).
 static tc_status spmv_host_enqueue(tc_plan *p, const float *h_x, float *h_y, int slot, cudaStream_t s)
 {
-    float *&dx = slot ? p->d_xbuf1 : p->d_xbuf;
-    float *&dy = slot ? p->d_ybuf1 : p->d_ybuf;
+    float *&dx = p->d_xbuf[slot];
+    float *&dy = p->d_ybuf[slot];
     if (!dx) {
         cudaError_t e1 = cudaMalloc(&dx, sizeof(float) * ((size_t)p->N + 4));
         cudaError_t e2 = cudaMalloc(&dy, sizeof(float) * ((size_t)p->M + 4));
@@ -281,8 +281,8 @@ tc_status tc_spmv_host(const tc_plan *cp, const float *h_x, float *h_y, void *st
 tc_status tc_spmv_host_async(const tc_plan *cp, const float *h_x, float *h_y, int slot, void *stream)
 {
     tc_plan *p = const_cast<tc_plan *>(cp);
-    if (!p || (!h_x && p->N) || (!h_y && p->M) || slot < 0 || slot > 1)
-        return fail(TC_ERR_INVALID, "tc_spmv_host_async: null argument or slot not 0/1");
+    if (!p || (!h_x && p->N) || (!h_y && p->M) || slot < 0 || slot >= TC_HOST_SLOTS)
+        return fail(TC_ERR_INVALID, "tc_spmv_host_async: null argument or slot outside [0, %d)", TC_HOST_SLOTS);
     return spmv_host_enqueue(p, h_x, h_y, slot, (cudaStream_t)stream);
 }
 

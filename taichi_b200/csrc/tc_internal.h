@@ -204,8 +204,9 @@ struct tc_plan {
     std::vector<unsigned char> thumb_stages;   // 5*H*W when kept
     std::vector<int> corners;                   // 4 per kept contour
     // device staging for tc_spmv_host
-    float *d_xbuf = nullptr, *d_ybuf = nullptr;     // slot 0
-    float *d_xbuf1 = nullptr, *d_ybuf1 = nullptr;   // slot 1 (tc_spmv_host_async)
+    // host-vector staging slots (tc_spmv_host: slot 0; tc_spmv_host_async:
+    // any of TC_HOST_SLOTS)
+    float *d_xbuf[TC_HOST_SLOTS] = {}, *d_ybuf[TC_HOST_SLOTS] = {};
 
     tc::DevPlan dev_plan() const;
     int64_t spmv_bytes() const;

@@ -252,26 +252,31 @@ def test_spmv_host_e2e(tc, dev):
     np.testing.assert_array_equal(y.astype(np.float64), oracle.spmv_csr_f64(M, rp, col, x.astype(np.float64)))
 
 
-def test_spmv_host_async_two_slots(tc, dev):
-    """Pipelined host multiplies: six requests alternate two staging slots on
-    two streams; each y equals the oracle's (integer x: exact)."""
+@pytest.mark.parametrize("slots", [2, 4])
+def test_spmv_host_async_slots(tc, dev, slots):
+    """Pipelined host multiplies: twelve requests rotate over 2 or 4 staging
+    slots on as many streams; each y equals the oracle's (integer x:
+    exact).  A slot outside [0, 4) is refused."""
     import torch
     M, N, rp, col = cases.matrix(cases.MATRIX_CASES[1])
     plan = tc.Plan.from_csr(M, N, rp, col)
     rng = np.random.default_rng(5)
-    xs = [torch.from_numpy(rng.integers(-8, 9, N).astype(np.float32)).pin_memory() for _ in range(6)]
-    ys = [torch.full((M,), float("nan")).pin_memory() for _ in range(6)]
-    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
-    for i in range(6):
-        plan.spmv_host_async(xs[i], ys[i], i & 1, streams[i & 1])
+    n = 12
+    xs = [torch.from_numpy(rng.integers(-8, 9, N).astype(np.float32)).pin_memory() for _ in range(n)]
+    ys = [torch.full((M,), float("nan")).pin_memory() for _ in range(n)]
+    streams = [torch.cuda.Stream(dev) for _ in range(slots)]
+    for i in range(n):
+        plan.spmv_host_async(xs[i], ys[i], i % slots, streams[i % slots])
     for s in streams:
         s.synchronize()
     plan.check()
-    for i in range(6):
+    for i in range(n):
         want = oracle.spmv_csr_f64(M, rp, col, xs[i].numpy().astype(np.float64))
         np.testing.assert_array_equal(ys[i].numpy().astype(np.float64), want, err_msg="request %d" % i)
     with pytest.raises(tc.TcError):
-        plan.spmv_host_async(xs[0], ys[0], 2, streams[0])
+        plan.spmv_host_async(xs[0], ys[0], 4, streams[0])
+    with pytest.raises(tc.TcError):
+        plan.spmv_host_async(xs[0], ys[0], -1, streams[0])
     plan.close()
 
 
