@@ -30,6 +30,19 @@ def test_thumbnail_entries_check_params_first(tc):
         assert st == TC_ERR_INVALID, (over, st)
 
 
+def test_plan_params_refused_before_cuda(tc):
+    """tc_params the multiply cannot honour are refused by the plan entry
+    points before any CUDA call: a rows-kernel word count outside {0, 4, 6,
+    8}, tile_mode 3, max_lanes 3."""
+    f = tc.Format()
+    out = C.c_void_p()
+    for over in ({"rows_w": 5}, {"rows_w": 16}, {"tile_mode": 3}, {"max_lanes": 3}):
+        p = tc.params(**over)
+        st = tc.lib().tc_plan_from_format(10, 10, C.byref(f), C.byref(p), None, C.byref(out))
+        assert st == TC_ERR_INVALID, (over, st)
+        assert "rows_w" in tc.lib().tc_last_error().decode() or "rows_w" not in over
+
+
 CACHE_TEST = r'''
 #include <cstdio>
 #include "tc_ctxcache.h"
