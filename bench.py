@@ -447,7 +447,7 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
         }
         if world == 1 and not args.no_forms and not over and args.workload == "rmat20":
-            # the north star's other forms, each measured on its own workload
+            # the batched, served and SpMM forms, each measured on its own workload
             # with its own clocks record (GPU 0 only; replicas runs skip them)
             for p in plans:
                 p.close()

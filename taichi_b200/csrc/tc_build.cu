@@ -67,9 +67,9 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist(const unsigned *__res
 }
 
 // Stable scatter of one digit pass: each block walks its tile in index order
-// (rounds of 256 records); a record's slot is its block's first slot for its
-// digit, plus the records of that digit in earlier rounds, earlier warps of
-// this round, and earlier lanes of its warp.
+// (steps of 256 records); a record's slot is its block's first slot for its
+// digit, plus the records of that digit in earlier steps, earlier warps of
+// this step, and earlier lanes of its warp.
 __global__ void __launch_bounds__(kSortThreads) radix_scatter(const unsigned *__restrict__ key_in,
                                                               const unsigned *__restrict__ idx_in, long n,
                                                               int shift, const unsigned *__restrict__ offs,
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const unsigned *__
 {
     constexpr int kWarps = kSortThreads / 32;
     __shared__ unsigned slot[kRadix];                // next slot of each digit
-    __shared__ unsigned wcnt[kWarps][kRadix];        // this round's count per warp and digit
+    __shared__ unsigned wcnt[kWarps][kRadix];        // this step's count per warp and digit
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     slot[threadIdx.x] = offs[(long)threadIdx.x * gridDim.x + blockIdx.x];
     const long base = (long)blockIdx.x * kSortTile;
