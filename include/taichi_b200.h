@@ -103,6 +103,14 @@ typedef struct tc_params {
 #define TC_FLAG_WINDOW       0x80 /* tile_mode 2: run the window kernel
                                      whenever the rows fit its tiles, even
                                      where the planner would not choose it   */
+#define TC_FLAG_HOST_Y_MAPPED 0x8000 /* tc_spmv_host / tc_spmv_host_async:
+                                     when h_y is page-locked host memory
+                                     the GPU can address (cudaHostAlloc,
+                                     cudaMallocHost, mapped registrations),
+                                     the multiply stores y straight into it
+                                     over the host link instead of into a
+                                     device buffer that a copy then reads
+                                     back; other h_y take the copy          */
 
 TC_API void tc_params_default(tc_params *p);
 
@@ -217,6 +225,10 @@ TC_API tc_status tc_spmv_host(const tc_plan *plan, const float *h_x, float *h_y,
  * between streams); slots on separate streams let one call's x copy-in
  * overlap another's y copy-out, and with three or more a copy-in no longer
  * waits for the copy-out two calls back.
+ * With TC_FLAG_HOST_Y_MAPPED and a page-locked, device-addressable h_y the
+ * multiply itself writes h_y (no copy-out and no device y buffer); h_y must
+ * then stay allocated, and unread and unwritten by the host, until the
+ * stream has passed this call, as for the copy.
  * No counterpart in the reference (its taichi_SpMV copies synchronously,
  * TaiChi.cu:1357-1420). */
 TC_API tc_status tc_spmv_host_async(const tc_plan *plan, const float *h_x, float *h_y, int slot,

@@ -30,6 +30,7 @@ TC_FLAG_ROWS = 0x400
 TC_FLAG_NO_ROWS = 0x800
 TC_FLAG_NO_PREFETCH = 0x2000
 TC_FLAG_NO_PARAM_STARTS = 0x4000
+TC_FLAG_HOST_Y_MAPPED = 0x8000
 
 _IP = C.POINTER(C.c_int)
 

@@ -251,18 +251,41 @@ tc_status tc_spmv(const tc_plan *p, const float *d_x, float *d_y, void *stream)
     return tc::launch_plan(p, d_x, d_y, (cudaStream_t)stream);
 }
 
+// The device address through which a kernel may store into h_y, or null when
+// h_y is not page-locked host memory mapped for the current device (pageable
+// memory, device memory, or a registration without a device mapping).
+static float *mapped_host_y(float *h_y)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, h_y) != cudaSuccess) {
+        cudaGetLastError();                  // an unknown pointer: not an error of this call
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<float *>(a.devicePointer) : nullptr;
+}
+
 // Copy x in, multiply, copy y out on `stream`, through the plan's staging
-// slot `slot` (device x / y buffers allocated on first use).
+// slot `slot` (device x / y buffers allocated on first use).  With
+// TC_FLAG_HOST_Y_MAPPED and a mapped page-locked h_y the multiply stores y
+// into h_y itself (every kernel writes y with plain stores only) and there
+// is no copy-out; a plan without columns keeps the copy (its y = 0 is a
+// device memset).
 static tc_status spmv_host_enqueue(tc_plan *p, const float *h_x, float *h_y, int slot, cudaStream_t s)
 {
+    float *yk = nullptr;
+    if ((p->params.flags & TC_FLAG_HOST_Y_MAPPED) && p->M && p->N) yk = mapped_host_y(h_y);
     float *&dx = p->d_xbuf[slot];
     float *&dy = p->d_ybuf[slot];
     if (!dx) {
         cudaError_t e1 = cudaMalloc(&dx, sizeof(float) * ((size_t)p->N + 4));
+        if (e1 != cudaSuccess) return fail(TC_ERR_ALLOC, "x staging buffer");
+    }
+    if (!dy && !yk) {
         cudaError_t e2 = cudaMalloc(&dy, sizeof(float) * ((size_t)p->M + 4));
-        if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(TC_ERR_ALLOC, "x/y staging buffers");
+        if (e2 != cudaSuccess) return fail(TC_ERR_ALLOC, "y staging buffer");
     }
     if (p->N) TC_CUDA(cudaMemcpyAsync(dx, h_x, sizeof(float) * (size_t)p->N, cudaMemcpyHostToDevice, s));
+    if (yk) return tc::launch_plan(p, dx, yk, s);
     TC_CHECK(tc::launch_plan(p, dx, dy, s));
     if (p->M) TC_CUDA(cudaMemcpyAsync(h_y, dy, sizeof(float) * (size_t)p->M, cudaMemcpyDeviceToHost, s));
     return TC_OK;

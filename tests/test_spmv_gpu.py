@@ -280,6 +280,75 @@ def test_spmv_host_async_slots(tc, dev, slots):
     plan.close()
 
 
+MAPPED_CASES = [("rmat20", {}), ("cfg1_small", {}), ("cfg1_small", {"flags": 0x80}),
+                ("band_holes", {"tile_mode": 0}), ("band_holes", {"tile_mode": 1}),
+                ("multi_shape", {}), ("rect_cols", {}), ("rmat16_selfloops", {})]
+
+
+@pytest.mark.parametrize("name,over", MAPPED_CASES,
+                         ids=["%s-%s" % (n, "-".join("%s%s" % kv for kv in o.items()) or "default")
+                              for n, o in MAPPED_CASES])
+def test_spmv_host_mapped_y(tc, dev, name, over):
+    """TC_FLAG_HOST_Y_MAPPED: the multiply stores y straight into a pinned
+    host buffer.  For each kernel kind, y is bit-identical to the device
+    multiply of the same plan and, for integer x, to the oracle -- through
+    tc_spmv_host and tc_spmv_host_async on two slots, into an aligned pinned
+    buffer, a pinned buffer one float off 16-byte alignment, and pageable
+    memory (which takes the copy)."""
+    import torch
+    case = next(c for c in cases.MATRIX_CASES if c["name"] == name)
+    M, N, rp, col = cases.matrix(case)
+    over = dict(over)
+    over["flags"] = over.get("flags", 0) | tc.TC_FLAG_HOST_Y_MAPPED
+    plan = tc.Plan.from_csr(M, N, rp, col, prm=tc.params(**over))
+    rng = np.random.default_rng(11)
+    xi = rng.integers(-8, 9, N).astype(np.float32)
+    xf = rng.uniform(-1, 1, N).astype(np.float32)
+    want_i = oracle.spmv_csr_f64(M, rp, col, xi.astype(np.float64))
+    dev_f = run_spmv(plan, xf, M, dev)
+    # the device multiply into a y one float off 16-byte alignment: the
+    # kernel path an unaligned host y takes
+    yoff = torch.full((M + 1,), float("nan"), device=dev)
+    plan.spmv(to_dev(xf, dev), yoff[1:])
+    torch.cuda.synchronize()
+    dev_f_off = yoff[1:].cpu().numpy()
+    for x, want, label in ((xi, want_i, "integer x"), (xf, None, "fp32 x")):
+        hx = torch.from_numpy(x).pin_memory()
+        pinned = torch.full((M + 1,), float("nan")).pin_memory()
+        targets = {"pinned": pinned[:M], "pinned+1": pinned[1:], "pageable": np.full(M, np.nan, np.float32)}
+        for tname, hy in targets.items():
+            plan.spmv_host(hx, hy)
+            got = hy.numpy() if hasattr(hy, "numpy") else hy
+            if want is not None:
+                np.testing.assert_array_equal(got.astype(np.float64), want, err_msg="%s %s %s" % (name, label, tname))
+            else:
+                np.testing.assert_array_equal(got, dev_f_off if tname == "pinned+1" else dev_f,
+                                              err_msg="%s %s %s" % (name, label, tname))
+        ys = [torch.full((M,), float("nan")).pin_memory() for _ in range(4)]
+        streams = [torch.cuda.Stream(dev) for _ in range(2)]
+        for i in range(4):
+            plan.spmv_host_async(hx, ys[i], i % 2, streams[i % 2])
+        for s in streams:
+            s.synchronize()
+        plan.check()
+        for i in range(4):
+            np.testing.assert_array_equal(ys[i].numpy(), targets["pinned"].numpy(), err_msg="%s async %d" % (name, i))
+    plan.close()
+
+
+def test_spmv_host_mapped_y_no_columns(tc, dev):
+    """A plan with rows but no columns keeps the copy under
+    TC_FLAG_HOST_Y_MAPPED: y = 0 in a pinned buffer."""
+    import torch
+    rp = np.zeros(9, np.int32)
+    plan = tc.Plan.from_csr(8, 0, rp, np.zeros(0, np.int32),
+                            prm=tc.params(flags=tc.TC_FLAG_HOST_Y_MAPPED), partition=False)
+    hy = torch.full((8,), float("nan")).pin_memory()
+    plan.spmv_host(np.zeros(1, np.float32), hy)
+    np.testing.assert_array_equal(hy.numpy(), np.zeros(8, np.float32))
+    plan.close()
+
+
 def test_format_rejected(tc):
     M, N = 10, 10
     rp = np.array([0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10], np.int32)
