@@ -13,9 +13,11 @@ resident in HBM; the timed region replays a CUDA graph of back-to-back SpMVs
 that rotate over enough resident copies of the matrix and vectors (> 2x the
 126 MB L2) that every SpMV reads its operands from HBM.  `e2e` is the same
 metric through the host-vector API: every step copies its x in from pinned
-host memory and its y out; steps alternate two staging slots on two streams
-(tc_spmv_host_async), so one step's copy-in overlaps the previous step's
-copy-out; `e2e.sync_value` is the synchronous tc_spmv_host, one step at a time.
+host memory and gets its y out, through tc_spmv_host_async with 2-4 staging
+slots on as many streams, y either copied out ("copy") or stored by the
+multiply straight into the pinned buffer ("mapped", TC_FLAG_HOST_Y_MAPPED);
+the fastest (form, slots) is the headline and all are listed;
+`e2e.sync_value` is the synchronous tc_spmv_host, one step at a time.
 With --impl reference the reference's CPU SpMV loop (main.cu:61-69, restated
 in the oracle) runs on all host cores on the same matrix.
 
@@ -366,42 +368,46 @@ def run_ours(args, rank, world, local_rank):
 
     # end to end through the public host API (pinned host buffers): every step
     # copies its x in and gets its y out.  Two forms of the same call,
-    # tc_spmv_host_async with --e2e-slots staging slots on as many streams:
-    # "copy" (the multiply writes a device y, a copy brings it out) and
-    # "mapped" (a plan with TC_FLAG_HOST_Y_MAPPED: the multiply stores y
-    # straight into the pinned host buffer over the host link).  The headline
-    # is the faster of the two on this box; both are reported, and the
-    # synchronous tc_spmv_host of each beside them.
-    S = args.e2e_slots
-    streams = [stream] + [torch.cuda.Stream(dev) for _ in range(S - 1)]
-    hxs = [torch.from_numpy(x_host).pin_memory() for _ in range(S)]
-    e2e_steps = max(3, min(args.steps, 400))
+    # tc_spmv_host_async with S staging slots on as many streams: "copy" (the
+    # multiply writes a device y, a copy brings it out) and "mapped" (a plan
+    # with TC_FLAG_HOST_Y_MAPPED: the multiply stores y straight into the
+    # pinned host buffer over the host link).  Each form runs with S = 2, 3
+    # and 4 slots (or --e2e-slots alone), 400 pipelined calls each; the
+    # headline is the fastest (form, S) on this box, and every pair is
+    # reported, with the synchronous tc_spmv_host of each form beside them.
+    slot_counts = [args.e2e_slots] if args.e2e_slots else [2, 3, 4]
+    Smax = max(slot_counts)
+    streams = [stream] + [torch.cuda.Stream(dev) for _ in range(Smax - 1)]
+    hxs = [torch.from_numpy(x_host).pin_memory() for _ in range(Smax)]
+    hys = [torch.empty(M, dtype=torch.float32).pin_memory() for _ in range(Smax)]
+    e2e_steps = 400
     plan_m = tc.Plan.from_format(M, N, fmt, prm=tc.params(**dict(over, flags=over.get("flags", 0) |
                                                                   tc.TC_FLAG_HOST_Y_MAPPED)), stream=stream)
-    e2e_forms = {}
+    e2e_forms, e2e_y = {}, {}
     for form, pl in (("copy", plan0), ("mapped", plan_m)):
-        hys = [torch.empty(M, dtype=torch.float32).pin_memory() for _ in range(S)]
         for _ in range(3):
             pl.spmv_host(hxs[0], hys[0], stream=stream)
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             pl.spmv_host(hxs[0], hys[0], stream=stream)
         sync_s = (time.perf_counter() - t0) / e2e_steps
-        for i in range(2 * S):
-            pl.spmv_host_async(hxs[i % S], hys[i % S], i % S, streams[i % S])
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for i in range(e2e_steps):
-            pl.spmv_host_async(hxs[i % S], hys[i % S], i % S, streams[i % S])
-        for s in streams:
-            s.synchronize()
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
-        pl.check()
-        for k in range(1, S):
-            assert np.array_equal(hys[0].numpy(), hys[k].numpy()), "pipelined host multiply mismatch"
-        e2e_forms[form] = {"gbs": bytes_per / e2e_s / 1e9 * world, "ms": e2e_s * 1e3,
-                           "sync_gbs": bytes_per / sync_s / 1e9 * world, "y": hys[0].numpy().copy()}
-    assert np.array_equal(e2e_forms["copy"]["y"], e2e_forms["mapped"]["y"]), "mapped-y multiply mismatch"
+        for S in slot_counts:
+            for i in range(2 * S):
+                pl.spmv_host_async(hxs[i % S], hys[i % S], i % S, streams[i % S])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for i in range(e2e_steps):
+                pl.spmv_host_async(hxs[i % S], hys[i % S], i % S, streams[i % S])
+            for st_ in streams[:S]:
+                st_.synchronize()
+            e2e_s = (time.perf_counter() - t0) / e2e_steps
+            pl.check()
+            for k in range(1, S):
+                assert np.array_equal(hys[0].numpy(), hys[k].numpy()), "pipelined host multiply mismatch"
+            e2e_forms["%s/%d" % (form, S)] = {"gbs": bytes_per / e2e_s / 1e9 * world, "ms": e2e_s * 1e3,
+                                              "sync_gbs": bytes_per / sync_s / 1e9 * world}
+        e2e_y[form] = hys[0].numpy().copy()
+    assert np.array_equal(e2e_y["copy"], e2e_y["mapped"]), "mapped-y multiply mismatch"
     plan_m.close()
     e2e_best = max(e2e_forms, key=lambda f: e2e_forms[f]["gbs"])
     e2e_gbs = e2e_forms[e2e_best]["gbs"]
@@ -452,7 +458,9 @@ def run_ours(args, rank, world, local_rank):
                          "peak_kind": peak_kind + " hbm_gbs (copy)", "traffic": traffic},
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 4 * N,
                     "d2h_bytes_per_step": 4 * M, "ms_per_step": e2e_s * 1e3,
-                    "api": "tc_spmv_host_async, %d slots on %d streams, %s form" % (S, S, e2e_best),
+                    "api": "tc_spmv_host_async, %s form, %s slots on as many streams" % tuple(
+                        e2e_best.split("/")),
+                    "steps": e2e_steps,
                     "forms": {f: {"value": round(v["gbs"], 3), "ms_per_step": round(v["ms"], 4),
                                   "sync_value": round(v["sync_gbs"], 3)} for f, v in e2e_forms.items()},
                     "sync_value": round(e2e_sync_gbs, 3), "sync_api": "tc_spmv_host"},
@@ -736,8 +744,9 @@ def main():
     ap.add_argument("--rows", action="store_true", help="stream plans: the rows kernel whatever the row lengths")
     ap.add_argument("--no-rows", action="store_true", help="stream plans: never the rows kernel")
     ap.add_argument("--rows-w", type=int, default=None, help="the rows kernel: words of a row loaded together")
-    ap.add_argument("--e2e-slots", type=int, default=4, choices=[1, 2, 3, 4],
-                    help="end-to-end figure: staging slots (and streams) of tc_spmv_host_async")
+    ap.add_argument("--e2e-slots", type=int, default=None, choices=[1, 2, 3, 4],
+                    help="end-to-end figure: staging slots (and streams) of tc_spmv_host_async "
+                         "(default: 2, 3 and 4, the fastest reported)")
     ap.add_argument("--no-param-starts", action="store_true",
                     help="wide plans: tile word ranges for the prefetch from the tile records")
     ap.add_argument("--no-prefetch", action="store_true",
