@@ -31,6 +31,18 @@ def test_c_symbols_exported(tc):
     assert set(tc.EXPORTS) <= set(syms)
 
 
+def test_flag_values_match_header(tc):
+    """Every TC_FLAG_* of the C header has the same value in the Python view,
+    and no two flags share a bit."""
+    text = open(os.path.join(ROOT, "include", "taichi_b200.h")).read()
+    flags = {k: int(v, 16) for k, v in re.findall(r"#define\s+(TC_FLAG_\w+)\s+(0x[0-9a-fA-F]+)", text)}
+    assert "TC_FLAG_HOST_Y_MAPPED" in flags and len(flags) >= 15
+    for k, v in flags.items():
+        assert getattr(tc, k) == v, k
+        assert v & (v - 1) == 0, k
+    assert len(set(flags.values())) == len(flags)
+
+
 def test_cpp_compat_symbols_exported(tc):
     out = subprocess.run(["nm", "-D", "--defined-only", "-C", tc.LIB_PATH],
                          stdout=subprocess.PIPE, text=True, check=True).stdout
