@@ -265,9 +265,11 @@ __global__ void __launch_bounds__(kDirectWideBlock, 2) spmv_wide_kernel(DevPlan 
     if (FULL) {
         wide_full<SIGNED, POS>(p, x, y, -1, -1);
     } else {
+        // the edge path (direct_run) has no one-diagonal shortcut: every plan's
+        // diagonal terms come from the tile's class
         const int row0 = blockIdx.x * p.wide_rows;
         const int nr = min(p.wide_rows, p.M - row0);
-        const int dc = SIGNED && p.dn != 1 ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
+        const int dc = SIGNED ? tile_dclass(p.tiles[blockIdx.x]) : kDiagNone;
         if (threadIdx.x == 0) prefetch_x_window(x, p.N, row0, nr);
         direct_run<SIGNED>(p, row0, nr, dc, x, y, true, 4 * threadIdx.x);
     }

@@ -681,3 +681,37 @@ def test_stream_rows_multiple_of_8(tc, dev, k, r):
     plan = tc.Plan.from_csr(n, n, rp, col, prm=tc.params(tile_mode=1, max_lanes=1), partition=False)
     np.testing.assert_array_equal(run_spmv(plan, x, n, dev), y)
     plan.close()
+
+
+@pytest.mark.parametrize("n,off,keep", [(300000, 0, 1.0), (300001, 6, 0.98), (299998, -3, 1.0)])
+def test_single_diagonal_edge_path(tc, dev, n, off, keep):
+    """One-diagonal wide plans on the wide kernel's edge path: x and y one
+    float off 16-byte alignment, and row counts that are not a multiple of
+    4.  Each y equals the oracle's for integer x and is bit-identical to the
+    aligned multiply for FP32 x (the diagonal terms come from the tile
+    classes there, from the launch parameters on the aligned path)."""
+    import torch
+    M, N, rp, col = matgen.segments(n, [(0, n, off, 0, keep)], noise=n // 5, seed=6)
+    fmt, _ = oracle.partition(M, N, rp, col)
+    assert fmt["dia_shapes"] == 1 and fmt["num_negs"] == 1, (fmt["dia_shapes"], fmt["num_negs"])
+    plan = tc.Plan.from_format(M, N, fmt)
+    rng = np.random.default_rng(3)
+    xi = rng.integers(-8, 9, N).astype(np.float32)
+    xf = rng.uniform(-1, 1, N).astype(np.float32)
+    want = oracle.spmv_csr_f64(M, rp, col, xi.astype(np.float64))
+    y_aligned = run_spmv(plan, xf, M, dev)
+    for xshift, yshift in ((0, 1), (1, 0), (1, 1)):
+        for x, label in ((xi, "integer"), (xf, "fp32")):
+            xb = torch.zeros(N + 1, device=dev)
+            xb[xshift:xshift + N] = torch.from_numpy(x).to(dev)
+            yb = torch.full((M + 1,), float("nan"), device=dev)
+            plan.spmv(xb[xshift:xshift + N], yb[yshift:yshift + M])
+            torch.cuda.synchronize()
+            plan.check()
+            got = yb[yshift:yshift + M].cpu().numpy()
+            msg = "n=%d off=%d x+%d y+%d %s" % (n, off, xshift, yshift, label)
+            if label == "integer":
+                np.testing.assert_array_equal(got.astype(np.float64), want, err_msg=msg)
+            else:
+                np.testing.assert_array_equal(got, y_aligned, err_msg=msg)
+    plan.close()
