@@ -165,6 +165,16 @@ def run_reference(args, rank):
                                        "rows split over %d OpenMP threads)" % (args.steps, threads)},
             "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    # the partition on the host, as the reference runs it (partition_shapes,
+    # TaiChi.cu:313-612, with getSdf's thumbnail, morphology and contours):
+    # one whole partition of the workload by the oracle's sequential
+    # restatement, beside the GPU partitioner's partition_ms of the other arm
+    t0 = time.perf_counter()
+    fmt, _ = oracle.partition(M, N, rp, col)
+    line["partition_baseline"] = {"ms": round((time.perf_counter() - t0) * 1e3, 1), "cores": 1,
+                                  "kind": "port", "dia_shapes": int(fmt["dia_shapes"]),
+                                  "sample": "one partition_shapes of the workload (oracle restatement, "
+                                            "sequential)"}
     if args.workload in ("rmat20", "small") and os.path.exists("/dev/nvidiactl") and not args.no_ref_gpu:
         line["reference_gpu"] = reference_gpu(args.workload)
     print(json.dumps(line), flush=True)
