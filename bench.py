@@ -449,7 +449,12 @@ def run_ours(args, rank, world, local_rank):
                        "dia_shapes": info["dia_shapes"], "num_negs": info["num_negs"],
                        "nnz_csr": info["nnz_csr"], "tiles": info["ntiles"], "kernel": tc.KERNEL_NAMES.get(info["kernel"]), "tile_mode": prm.tile_mode, "tile_rows": prm.tile_rows,
                        "tile_nnz": prm.tile_nnz, "flags": prm.flags,
-                       "bytes_per_spmv": bytes_per, "format_build_s": round(build_s, 3),
+                       "bytes_per_spmv": bytes_per,
+                       # the same time over the plain-CSR bytes of the matrix
+                       # (row pointers, every entry's column, x, y)
+                       "effective_csr_gbs": round(gbs * (4 * (M + 1) + 4 * int(rp[M]) + 4 * N + 4 * M)
+                                                  / bytes_per, 2),
+                       "format_build_s": round(build_s, 3),
                        "partition_ms": info["partition_ms"],
                        "timing": ("one CUDA graph: %d untimed SpMVs, %d timed, %d untimed; events are "
                                   "graph nodes on a side branch after the last untimed and the last timed "
